@@ -1,0 +1,159 @@
+/*
+ * gpz_b200.h -- C ABI of the B200-native GPZ particle compressor.
+ *
+ * Plain C: pointers, sizes and status codes only.  Device pointers are CUDA
+ * global-memory addresses on the current device; `stream` is a cudaStream_t
+ * passed as void* (NULL = legacy default stream).  Every entry point returns
+ * GPZ_OK (0) or one of the GPZ_E* codes below and never exits the process.
+ *
+ * The compressed stream is byte-compatible with the GPZ reference format:
+ * header, per-chunk offset table, per-chunk meta records and bit-plane
+ * payloads for 1024-point chunks (reference src/cudaWarpCompress.cu:1668-1702,
+ * src/cudaWarpCompressDouble.cu:1670-1702).
+ *
+ * Each entry point names the reference interface it replaces (path:line in
+ * the GPZ project).  The C++ drop-in classes with the reference's own names
+ * (ICudaCompressor, CudaWarpCompress, CudaWarpCompressDouble,
+ * CompressorManager, CudaConfig) are declared in include/gpz/ and sit on top
+ * of this ABI.
+ */
+#ifndef GPZ_B200_H
+#define GPZ_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes -------------------------------------------------------- */
+#define GPZ_OK 0
+#define GPZ_EINVAL 1      /* bad argument (null pointer, dim, float_bits, seg 0 in abs mode ...) */
+#define GPZ_ESEG 2        /* auto segment size would exceed 1024 (reference: exit(1),
+                             src/cudaWarpCompress.cu:1547-1550) */
+#define GPZ_ESTREAM 3     /* malformed or truncated compressed stream */
+#define GPZ_ENOSPACE 4    /* output or scratch buffer too small */
+#define GPZ_ECUDA 5       /* a CUDA runtime call failed */
+#define GPZ_ETIMEOUT 6    /* a bounded device-side wait gave up (kernel returned early) */
+#define GPZ_ENOTSUP 7     /* feature not compiled in (e.g. nvcomp back-ends) */
+
+/* ---- parameters ------------------------------------------------------------
+ * Mirrors CudaConfig (reference include/cudaCompress.cuh:16-40). */
+typedef struct gpz_params {
+  uint32_t float_bits; /* 32 or 64 (CudaConfig::float_bits) */
+  uint32_t dim;        /* 2 or 3 (CudaConfig::dim) */
+  uint64_t n;          /* number of points (CudaConfig::coordinate_num) */
+  double eb;           /* absolute error bound; rounded to float when float_bits == 32
+                          (CudaConfig::eb / eb_dbl) */
+  double rel_eb;       /* relative bound as given by the user; only read by the automatic
+                          segment-size rule (CudaConfig::rel_eb / rel_eb_dbl) */
+  int32_t rel_mode;    /* 1 when error_mode == "rel" (CudaConfig::error_mode) */
+  uint32_t seg_size;   /* 0 = automatic (CudaConfig::seg_size) */
+  uint32_t flags;      /* GPZ_FLAG_* */
+  uint32_t reserved;
+} gpz_params;
+
+/* Extension (not in the reference): also double the segment size until every
+ * block id fits in 31 bits, so the reference's 0x7FFFFFFF mask
+ * (src/cudaWarpCompress.cu:187-189) never truncates an id.  Streams stay in
+ * the reference format but differ from the reference's bytes when it fires. */
+#define GPZ_FLAG_SAFE31 1u
+
+/* Result of a compress / decompress call, read back from device scratch. */
+typedef struct gpz_result {
+  uint64_t stream_bytes; /* compressed size (compress) */
+  uint32_t seg_size;     /* resolved segment size (CudaConfig::seg_size after the call) */
+  uint32_t adjusted;     /* CudaConfig::adjusted_seg after the call */
+  int32_t status;        /* GPZ_OK or device-side error */
+  uint32_t id_overflow;  /* 1 if some block id exceeded 31 bits and was masked (reference quirk) */
+} gpz_result;
+
+/* ---- sizes ------------------------------------------------------------------ */
+
+/* Worst-case compressed size for n points (any data). */
+uint64_t gpz_stream_bound(uint64_t n, uint32_t dim, uint32_t float_bits);
+
+/* Device scratch needed by gpz_compress_async for n points (control block
+ * plus one 8-byte look-back word per 1024-point chunk).  Replaces the
+ * caller-provided 4*N*sizeof(T) scratch of ICudaCompressor::compress
+ * (reference include/ICudaCompressor.cuh:10-11, src/main.cpp:289-291). */
+uint64_t gpz_compress_scratch_bytes(uint64_t n);
+
+/* Device scratch needed by gpz_decompress_async. */
+uint64_t gpz_decompress_scratch_bytes(void);
+
+/* ---- compress ----------------------------------------------------------------
+ * Replaces CudaWarpCompress::compress / CudaWarpCompressDouble::compress
+ * (reference include/cudaWarpCompress.cuh:21-22, src/cudaWarpCompress.cu:1559-1741;
+ * src/cudaWarpCompressDouble.cu:1557-1741), reached through
+ * CompressorManager::compressWarp (src/CompressorManager.cpp:12-16).
+ *
+ * d_x, d_y, d_z: SoA coordinates (n values of float or double each; d_z is
+ * ignored for dim == 2).  d_out receives the complete stream (header, offset
+ * table, meta, payload); out_capacity is its size in bytes.  The inputs are
+ * not modified (the reference overwrites its input with the stream; the C++
+ * drop-in class keeps that behaviour).
+ *
+ * Enqueues everything on `stream` and returns without synchronising; host
+ * argument errors are returned immediately.  Device-side results (size,
+ * chosen segment size, status) land in the scratch control block and are
+ * read with gpz_result_get(). */
+int gpz_compress_async(const gpz_params *params, const void *d_x, const void *d_y,
+                       const void *d_z, void *d_out, uint64_t out_capacity,
+                       void *d_scratch, uint64_t scratch_bytes, void *stream);
+
+/* Synchronous form: gpz_compress_async + gpz_result_get.  `result` may be NULL. */
+int gpz_compress(const gpz_params *params, const void *d_x, const void *d_y, const void *d_z,
+                 void *d_out, uint64_t out_capacity, void *d_scratch, uint64_t scratch_bytes,
+                 gpz_result *result, void *stream);
+
+/* ---- decompress ----------------------------------------------------------------
+ * Replaces CudaWarpCompress::decompress / CudaWarpCompressDouble::decompress
+ * (reference include/cudaWarpCompress.cuh:24-25, src/cudaWarpCompress.cu:1743-1856),
+ * reached through CompressorManager::decompressWarp (src/CompressorManager.cpp:18-22).
+ *
+ * d_stream: the compressed stream on the device, stream_bytes long.
+ * float_bits must match the stream header (the caller reads it from its host
+ * copy with gpz_parse_header, as decompressLoadParas does).  Outputs are SoA,
+ * out_capacity points each; points come out in the stream's order (sorted by
+ * block within each 1024-point chunk), as in the reference.  d_z is ignored
+ * for 2D streams.  Header and every chunk record are validated on the device;
+ * a bad chunk sets GPZ_ESTREAM and is not written. */
+int gpz_decompress_async(const void *d_stream, uint64_t stream_bytes, uint32_t float_bits,
+                         void *d_x, void *d_y, void *d_z, uint64_t out_capacity,
+                         void *d_scratch, uint64_t scratch_bytes, void *stream);
+
+int gpz_decompress(const void *d_stream, uint64_t stream_bytes, uint32_t float_bits,
+                   void *d_x, void *d_y, void *d_z, uint64_t out_capacity, void *d_scratch,
+                   uint64_t scratch_bytes, gpz_result *result, void *stream);
+
+/* Reads the control block written by the last call that used d_scratch
+ * (synchronises `stream`). */
+int gpz_result_get(const void *d_scratch, gpz_result *result, void *stream);
+
+/* ---- helpers -------------------------------------------------------------------- */
+
+/* Host-side header parse of a stream held in host memory.
+ * Replaces CompressorManager::decompressLoadParas (src/CompressorManager.cpp:24-34). */
+int gpz_parse_header(const void *h_stream, uint64_t bytes, uint32_t *dim, uint64_t *n,
+                     uint32_t *float_bits, double *eb, uint32_t *seg_size);
+
+/* Relative -> absolute error bound, computed on the device from the SoA input
+ * with the same arithmetic the reference CLI uses on the host
+ * (findMinimumValues<T>, include/utils.cuh:44-65; convertRelEb<T>,
+ * src/main.cpp:35-55).  For float_bits == 32 `rel` is rounded to float first
+ * (src/main.cpp:254).  Writes the absolute bound and the six min/max values
+ * (x_min, y_min, z_min, x_max, y_max, z_max; z = 0 for 2D) to host memory.
+ * Synchronises `stream`.  Needs gpz_compress_scratch_bytes(0) bytes of scratch. */
+int gpz_rel_to_abs(uint32_t float_bits, uint32_t dim, uint64_t n, const void *d_x,
+                   const void *d_y, const void *d_z, double rel, void *d_scratch,
+                   uint64_t scratch_bytes, double *h_eb, double *h_minmax6, void *stream);
+
+/* Library version string. */
+const char *gpz_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* GPZ_B200_H */
