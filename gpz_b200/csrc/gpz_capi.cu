@@ -1,0 +1,259 @@
+// gpz_capi.cu -- C ABI of the B200 GPZ codec (declared in include/gpz_b200.h).
+//
+// Host orchestration replacing CudaWarpCompress::compressImpl /
+// decompressImpl (reference src/cudaWarpCompress.cu:1573-1856 and the double
+// twin): no allocation, no host synchronisation and no small memcpys inside
+// the call -- one memset of the scratch control block, the sampling kernel
+// that resolves the segment size on the device, and one persistent
+// compress kernel that writes the finished stream.
+
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+
+#include "gpz_b200.h"
+#include "gpz_kernels.cuh"
+
+using namespace gpzb;
+
+namespace {
+
+int g_num_sms = 0;
+
+int num_sms() {
+  if (g_num_sms == 0) {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return 148;
+    if (cudaDeviceGetAttribute(&g_num_sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) g_num_sms = 148;
+  }
+  return g_num_sms;
+}
+
+template <typename K>
+int occupancy(K kernel) {
+  int blocks = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, kernel, kThreads, 0) != cudaSuccess || blocks < 1)
+    blocks = 1;
+  return blocks;
+}
+
+inline int cuda_status(cudaError_t e) { return e == cudaSuccess ? GPZ_OK : GPZ_ECUDA; }
+
+inline bool aligned16(const void *p) { return ((uintptr_t)p & 15u) == 0; }
+
+inline uint64_t chunks(uint64_t n) { return (n + kChunk - 1) / kChunk; }
+
+template <typename T>
+int compress_t(const gpz_params *p, const void *d_x, const void *d_y, const void *d_z, void *d_out,
+               uint64_t out_capacity, void *d_scratch, uint64_t scratch_bytes, cudaStream_t st) {
+  using Tr = TT<T>;
+  const uint64_t G = chunks(p->n);
+  if (out_capacity < Tr::hdr + G * (8ull + Tr::meta)) return GPZ_ENOSPACE;
+  if (scratch_bytes < gpz_compress_scratch_bytes(p->n)) return GPZ_ENOSPACE;
+  Control *ctl = static_cast<Control *>(d_scratch);
+  unsigned long long *look = reinterpret_cast<unsigned long long *>(static_cast<uint8_t *>(d_scratch) + kCtlBytes);
+  cudaError_t e = cudaMemsetAsync(d_scratch, 0, kCtlBytes + 8ull * G, st);
+  if (e != cudaSuccess) return GPZ_ECUDA;
+  const T eb = (T)p->eb;
+  const T rel = (T)p->rel_eb;
+  const T *x = static_cast<const T *>(d_x), *y = static_cast<const T *>(d_y), *z = static_cast<const T *>(d_z);
+  seg_sample_kernel<T><<<128, 256, 0, st>>>(x, y, p->dim == 3 ? z : y, p->n, p->dim, p->seg_size, p->rel_mode, rel,
+                                            eb, (p->flags & GPZ_FLAG_SAFE31) ? 1 : 0, ctl);
+  CArgs<T> a;
+  a.x = x; a.y = y; a.z = p->dim == 3 ? z : y;
+  a.out = static_cast<uint8_t *>(d_out);
+  a.out_cap = out_capacity;
+  a.ctl = ctl;
+  a.look = look;
+  a.n = p->n;
+  a.G = G;
+  a.eb = eb;
+  a.dim = p->dim;
+  a.vec_ok = aligned16(d_x) && aligned16(d_y) && (p->dim == 2 || aligned16(d_z));
+  if (p->dim == 3) {
+    static int occ = 0;
+    if (!occ) occ = occupancy(compress_kernel<T, 3>);
+    const uint64_t grid = std::min<uint64_t>(G, (uint64_t)num_sms() * occ);
+    compress_kernel<T, 3><<<(unsigned)grid, kThreads, 0, st>>>(a);
+  } else {
+    static int occ = 0;
+    if (!occ) occ = occupancy(compress_kernel<T, 2>);
+    const uint64_t grid = std::min<uint64_t>(G, (uint64_t)num_sms() * occ);
+    compress_kernel<T, 2><<<(unsigned)grid, kThreads, 0, st>>>(a);
+  }
+  return cuda_status(cudaGetLastError());
+}
+
+template <typename T>
+int decompress_t(const void *d_stream, uint64_t stream_bytes, uint32_t dim, void *d_x, void *d_y, void *d_z,
+                 uint64_t out_capacity, void *d_scratch, uint64_t scratch_bytes, cudaStream_t st) {
+  if (scratch_bytes < gpz_decompress_scratch_bytes()) return GPZ_ENOSPACE;
+  if (((uintptr_t)d_stream & 7u) != 0) return GPZ_EINVAL;
+  Control *ctl = static_cast<Control *>(d_scratch);
+  cudaError_t e = cudaMemsetAsync(d_scratch, 0, kCtlBytes, st);
+  if (e != cudaSuccess) return GPZ_ECUDA;
+  DArgs<T> a;
+  a.s = static_cast<const uint8_t *>(d_stream);
+  a.bytes = stream_bytes;
+  a.x = static_cast<T *>(d_x);
+  a.y = static_cast<T *>(d_y);
+  a.z = dim == 3 ? static_cast<T *>(d_z) : static_cast<T *>(d_y);
+  a.cap = out_capacity;
+  a.ctl = ctl;
+  a.vec_ok = aligned16(d_x) && aligned16(d_y) && (dim == 2 || aligned16(d_z));
+  // The chunk count lives in the device header; a grid of at most one full
+  // wave loops over however many chunks there are.
+  const uint64_t bound_chunks = stream_bytes / (8ull + TT<T>::meta) + 1;
+  if (dim == 3) {
+    static int occ = 0;
+    if (!occ) occ = occupancy(decompress_kernel<T, 3>);
+    const uint64_t grid = std::min<uint64_t>((uint64_t)num_sms() * occ, bound_chunks);
+    decompress_kernel<T, 3><<<(unsigned)grid, kThreads, 0, st>>>(a);
+  } else {
+    static int occ = 0;
+    if (!occ) occ = occupancy(decompress_kernel<T, 2>);
+    const uint64_t grid = std::min<uint64_t>((uint64_t)num_sms() * occ, bound_chunks);
+    decompress_kernel<T, 2><<<(unsigned)grid, kThreads, 0, st>>>(a);
+  }
+  return cuda_status(cudaGetLastError());
+}
+
+}  // namespace
+
+extern "C" {
+
+const char *gpz_version(void) { return "gpz_b200 0.1 (sm_100a)"; }
+
+uint64_t gpz_stream_bound(uint64_t n, uint32_t dim, uint32_t float_bits) {
+  (void)dim;
+  const uint64_t G = chunks(n);
+  const uint64_t hdr = float_bits == 64 ? 32 : 24, meta = float_bits == 64 ? 64 : 36;
+  return hdr + G * (8 + meta + 31 * 128 + 11 * 128 + 31 * 128 + 16);
+}
+
+uint64_t gpz_compress_scratch_bytes(uint64_t n) { return (uint64_t)kCtlBytes + 8ull * chunks(n); }
+
+uint64_t gpz_decompress_scratch_bytes(void) { return (uint64_t)kCtlBytes; }
+
+int gpz_compress_async(const gpz_params *p, const void *d_x, const void *d_y, const void *d_z, void *d_out,
+                       uint64_t out_capacity, void *d_scratch, uint64_t scratch_bytes, void *stream) {
+  if (!p || !d_x || !d_y || !d_out || !d_scratch) return GPZ_EINVAL;
+  if (p->dim != 2 && p->dim != 3) return GPZ_EINVAL;
+  if (p->dim == 3 && !d_z) return GPZ_EINVAL;
+  if (p->float_bits != 32 && p->float_bits != 64) return GPZ_EINVAL;
+  if (p->n == 0 || chunks(p->n) >= (1ull << 31)) return GPZ_EINVAL;
+  // abs mode without a segment size: the reference shifts by __ffs(0)-1 (UB)
+  if (p->seg_size == 0 && !p->rel_mode) return GPZ_EINVAL;
+  if (((uintptr_t)d_out & 7u) != 0 || ((uintptr_t)d_scratch & 15u) != 0) return GPZ_EINVAL;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  return p->float_bits == 32 ? compress_t<float>(p, d_x, d_y, d_z, d_out, out_capacity, d_scratch, scratch_bytes, st)
+                             : compress_t<double>(p, d_x, d_y, d_z, d_out, out_capacity, d_scratch, scratch_bytes, st);
+}
+
+int gpz_result_get(const void *d_scratch, gpz_result *result, void *stream) {
+  if (!d_scratch) return GPZ_EINVAL;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  gpz_result r;
+  memset(&r, 0, sizeof(r));
+  cudaError_t e = cudaMemcpyAsync(&r, d_scratch, sizeof(gpz_result), cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) return GPZ_ECUDA;
+  if (result) *result = r;
+  return r.status;
+}
+
+int gpz_compress(const gpz_params *p, const void *d_x, const void *d_y, const void *d_z, void *d_out,
+                 uint64_t out_capacity, void *d_scratch, uint64_t scratch_bytes, gpz_result *result, void *stream) {
+  int rc = gpz_compress_async(p, d_x, d_y, d_z, d_out, out_capacity, d_scratch, scratch_bytes, stream);
+  if (rc) return rc;
+  return gpz_result_get(d_scratch, result, stream);
+}
+
+int gpz_decompress_async(const void *d_stream, uint64_t stream_bytes, uint32_t float_bits, uint32_t dim, void *d_x,
+                         void *d_y, void *d_z, uint64_t out_capacity, void *d_scratch, uint64_t scratch_bytes,
+                         void *stream) {
+  if (!d_stream || !d_x || !d_y || !d_scratch) return GPZ_EINVAL;
+  if (float_bits != 32 && float_bits != 64) return GPZ_EINVAL;
+  if (dim != 2 && dim != 3) return GPZ_EINVAL;
+  if (dim == 3 && !d_z) return GPZ_EINVAL;
+  if (((uintptr_t)d_scratch & 15u) != 0) return GPZ_EINVAL;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  return float_bits == 32
+             ? decompress_t<float>(d_stream, stream_bytes, dim, d_x, d_y, d_z, out_capacity, d_scratch, scratch_bytes,
+                                   st)
+             : decompress_t<double>(d_stream, stream_bytes, dim, d_x, d_y, d_z, out_capacity, d_scratch,
+                                    scratch_bytes, st);
+}
+
+int gpz_decompress(const void *d_stream, uint64_t stream_bytes, uint32_t float_bits, uint32_t dim, void *d_x,
+                   void *d_y, void *d_z, uint64_t out_capacity, void *d_scratch, uint64_t scratch_bytes,
+                   gpz_result *result, void *stream) {
+  int rc = gpz_decompress_async(d_stream, stream_bytes, float_bits, dim, d_x, d_y, d_z, out_capacity, d_scratch,
+                                scratch_bytes, stream);
+  if (rc) return rc;
+  return gpz_result_get(d_scratch, result, stream);
+}
+
+int gpz_parse_header(const void *h_stream, uint64_t bytes, uint32_t *dim, uint64_t *n, uint32_t *float_bits,
+                     double *eb, uint32_t *seg_size) {
+  // CompressorManager::decompressLoadParas (src/CompressorManager.cpp:24-34):
+  // dim @0, N @4, float_bits @12; eb @16; seg @20 (f32) / @24 (f64).
+  if (!h_stream || bytes < 24) return GPZ_ESTREAM;
+  const uint8_t *s = static_cast<const uint8_t *>(h_stream);
+  uint32_t d, b, sg;
+  uint64_t nn;
+  memcpy(&d, s, 4);
+  memcpy(&nn, s + 4, 8);
+  memcpy(&b, s + 12, 4);
+  double e;
+  if (b == 32) {
+    float f;
+    memcpy(&f, s + 16, 4);
+    e = f;
+    memcpy(&sg, s + 20, 4);
+  } else if (b == 64) {
+    if (bytes < 32) return GPZ_ESTREAM;
+    memcpy(&e, s + 16, 8);
+    memcpy(&sg, s + 24, 4);
+  } else {
+    return GPZ_ESTREAM;
+  }
+  if ((d != 2 && d != 3) || nn == 0) return GPZ_ESTREAM;
+  if (dim) *dim = d;
+  if (n) *n = nn;
+  if (float_bits) *float_bits = b;
+  if (eb) *eb = e;
+  if (seg_size) *seg_size = sg;
+  return GPZ_OK;
+}
+
+int gpz_rel_to_abs(uint32_t float_bits, uint32_t dim, uint64_t n, const void *d_x, const void *d_y,
+                   const void *d_z, double rel, void *d_scratch, uint64_t scratch_bytes, double *h_eb,
+                   double *h_minmax6, void *stream) {
+  if (!d_x || !d_y || (dim == 3 && !d_z) || !d_scratch || n == 0) return GPZ_EINVAL;
+  if ((dim != 2 && dim != 3) || (float_bits != 32 && float_bits != 64)) return GPZ_EINVAL;
+  if (scratch_bytes < (uint64_t)kCtlBytes) return GPZ_ENOSPACE;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  Control *ctl = static_cast<Control *>(d_scratch);
+  if (cudaMemsetAsync(d_scratch, 0, kCtlBytes, st) != cudaSuccess) return GPZ_ECUDA;
+  const int grid = num_sms() * 4;
+  if (float_bits == 32)
+    rel_to_abs_kernel<float><<<grid, 256, 0, st>>>(static_cast<const float *>(d_x), static_cast<const float *>(d_y),
+                                                   static_cast<const float *>(dim == 3 ? d_z : d_y), n, dim,
+                                                   (float)rel, ctl);
+  else
+    rel_to_abs_kernel<double><<<grid, 256, 0, st>>>(static_cast<const double *>(d_x),
+                                                    static_cast<const double *>(d_y),
+                                                    static_cast<const double *>(dim == 3 ? d_z : d_y), n, dim, rel,
+                                                    ctl);
+  if (cudaGetLastError() != cudaSuccess) return GPZ_ECUDA;
+  Control h;
+  if (cudaMemcpyAsync(&h, d_scratch, sizeof(Control), cudaMemcpyDeviceToHost, st) != cudaSuccess) return GPZ_ECUDA;
+  if (cudaStreamSynchronize(st) != cudaSuccess) return GPZ_ECUDA;
+  if (h_eb) *h_eb = h.out_eb;
+  if (h_minmax6)
+    for (int k = 0; k < 6; ++k) h_minmax6[k] = h.out_mm[k];
+  return GPZ_OK;
+}
+
+}  // extern "C"

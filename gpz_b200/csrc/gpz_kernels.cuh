@@ -1,0 +1,1109 @@
+// gpz_kernels.cuh -- sm_100a kernels of the B200 GPZ codec.
+//
+//   seg_sample_kernel   computeSegSize (reference src/cudaWarpCompress.cu:1424-1557)
+//   rel_to_abs_kernel   findMinimumValues + convertRelEb (include/utils.cuh:44-65,
+//                       src/main.cpp:35-55), on the device
+//   compress_kernel     runCompressKernel[2D] + CUB scan + header/meta assembly +
+//                       runCompactKernel (src/cudaWarpCompress.cu:32-796, 1620-1702)
+//                       fused into one persistent, single-pass kernel
+//   decompress_kernel   runDecompressKernel[2D] (src/cudaWarpCompress.cu:798-1214)
+//
+// float64 twins: src/cudaWarpCompressDouble.cu (same line ranges +/- 3).
+#pragma once
+
+#include <cfloat>
+#include "gpz_device.cuh"
+
+namespace gpzb {
+
+// ===========================================================================
+// Automatic segment size (computeSegSize).
+// ===========================================================================
+// Host arithmetic of computeSegSize (src/cudaWarpCompress.cu:1488-1554),
+// evaluated on the device with explicitly rounded operations so no
+// contraction can differ from the reference's host build.
+__device__ void seg_decide(const float mm[6], uint32_t dim, uint32_t seg_in, int rel_mode,
+                           float rel_eb, float eb, int safe31, Control *ctl) {
+  const float dx = __fsub_rn(mm[3], mm[0]), dy = __fsub_rn(mm[4], mm[1]), dz = __fsub_rn(mm[5], mm[2]);
+  const float mean = __fdiv_rn(__fadd_rn(__fadd_rn(dx, dy), dz), 3.0f);
+  const float ex = __fsub_rn(dx, mean), ey = __fsub_rn(dy, mean), ez = __fsub_rn(dz, mean);
+  float var = __fadd_rn(__fadd_rn(__fmul_rn(ex, ex), __fmul_rn(ey, ey)), __fmul_rn(ez, ez));
+  var = __fdiv_rn(var, dim == 3 ? 3.0f : 2.0f);  // the float 2D path divides by 2 (:1503)
+  const float ratio = __fdiv_rn(__fsqrt_rn(var), mean);
+  const float maxr = fmaxf(fmaxf(dx, dy), dz);
+  uint32_t seg = seg_in;
+  if (seg == 0 && rel_mode) {
+    if (ratio < 0.1f) seg = ((double)rel_eb <= 1e-4) ? 32u : 2u;
+    else seg = ((double)rel_eb <= 1e-4) ? 4u : 1u;
+  }
+  if (seg == 0) { set_status(ctl, kEINVAL); return; }
+  const unsigned long long limit = safe31 ? 0x7FFFFFFFull : 0xFFFFFFFFull;
+  auto total = [&](uint32_t s) {
+    const unsigned long long mb =
+        __float2ull_rz(ceilf(__fdiv_rn(maxr, __fmul_rn(__uint2float_rn(2u * s), eb)))) + 1ull;
+    return dim == 3 ? mb * mb * mb : mb * mb;
+  };
+  uint32_t adj = 0;
+  if (total(seg) > limit) {
+    uint32_t t = seg;
+    for (int i = 0; i < 11; ++i) {
+      t *= 2u;
+      if (total(t) <= limit) break;
+    }
+    if (t > 1024u) { set_status(ctl, kESEG); return; }
+    seg = t;
+    adj = 1;
+  }
+  ctl->seg = seg;
+  ctl->adjusted = adj;
+}
+
+// Double twin (src/cudaWarpCompressDouble.cu:1488-1553): variance divides by 3
+// for 2D too, and the reference's overflow guard compares with UINT64_MAX and
+// never fires; only the 31-bit extension adjusts.
+__device__ void seg_decide(const double mm[6], uint32_t dim, uint32_t seg_in, int rel_mode,
+                           double rel_eb, double eb, int safe31, Control *ctl) {
+  const double dx = __dsub_rn(mm[3], mm[0]), dy = __dsub_rn(mm[4], mm[1]), dz = __dsub_rn(mm[5], mm[2]);
+  const double mean = __ddiv_rn(__dadd_rn(__dadd_rn(dx, dy), dz), 3.0);
+  const double ex = __dsub_rn(dx, mean), ey = __dsub_rn(dy, mean), ez = __dsub_rn(dz, mean);
+  double var = __dadd_rn(__dadd_rn(__dmul_rn(ex, ex), __dmul_rn(ey, ey)), __dmul_rn(ez, ez));
+  var = __ddiv_rn(var, 3.0);
+  const double ratio = __ddiv_rn(__dsqrt_rn(var), mean);
+  const double maxr = fmax(fmax(dx, dy), dz);
+  uint32_t seg = seg_in;
+  if (seg == 0 && rel_mode) {
+    if (ratio < (double)0.1f) seg = (rel_eb <= 1e-4) ? 32u : 2u;
+    else seg = (rel_eb <= 1e-4) ? 4u : 1u;
+  }
+  if (seg == 0) { set_status(ctl, kEINVAL); return; }
+  uint32_t adj = 0;
+  if (safe31) {
+    auto total = [&](uint32_t s) {
+      const unsigned long long mb =
+          __double2ull_rz(ceil(__ddiv_rn(maxr, __dmul_rn(__uint2double_rn(2u * s), eb)))) + 1ull;
+      return dim == 3 ? mb * mb * mb : mb * mb;
+    };
+    if (total(seg) > 0x7FFFFFFFull) {
+      uint32_t t = seg;
+      for (int i = 0; i < 11; ++i) {
+        t *= 2u;
+        if (total(t) <= 0x7FFFFFFFull) break;
+      }
+      if (t > 1024u) { set_status(ctl, kESEG); return; }
+      seg = t;
+      adj = 1;
+    }
+  }
+  ctl->seg = seg;
+  ctl->adjusted = adj;
+}
+
+template <typename T>
+__device__ __forceinline__ void fold_minmax(T v, typename TT<T>::U &mn_inv, typename TT<T>::U &mx) {
+  if (v == v) {
+    const typename TT<T>::U o = ord_of(v);
+    mn_inv = max(mn_inv, (typename TT<T>::U)~o);
+    mx = max(mx, o);
+  }
+}
+
+// sampleMinMaxXYZKernel[2D] + reduceMinMax[2D] (src/cudaWarpCompress.cu:1216-1418):
+// 1024 windows of 256 consecutive points at stride max((N-256)/1024, 1).
+// A window that would run past N is skipped by the reference and its
+// min/max slot keeps the zero-filled scratch value, so it contributes 0.0.
+// Launch: 128 blocks x 256 threads, 8 windows per block.  The last block to
+// finish applies the host decision rules (seg_decide).
+template <typename T>
+__global__ void __launch_bounds__(256) seg_sample_kernel(const T *__restrict__ x, const T *__restrict__ y,
+                                                         const T *__restrict__ z, uint64_t n, uint32_t dim,
+                                                         uint32_t seg_in, int rel_mode, T rel_eb, T eb,
+                                                         int safe31, Control *ctl) {
+  using U = typename TT<T>::U;
+  __shared__ U red[6][8];
+  __shared__ int last;
+  const unsigned long long L = 256, B = 1024;
+  const unsigned long long stride = max((n - L) / B, 1ull);
+  U acc[6] = {0, 0, 0, 0, 0, 0};  // [min_inv, max] per axis
+  const T *X[3] = {x, y, z};
+  for (int w = 0; w < 8; ++w) {
+    const unsigned long long win = (unsigned long long)blockIdx.x * 8 + w;
+    const unsigned long long st = win * stride;
+    if (st + L > n) {
+      for (uint32_t d = 0; d < dim; ++d) fold_minmax<T>((T)0, acc[2 * d], acc[2 * d + 1]);
+      continue;
+    }
+    for (uint32_t d = 0; d < dim; ++d) fold_minmax<T>(X[d][st + threadIdx.x], acc[2 * d], acc[2 * d + 1]);
+  }
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int k = 0; k < 6; ++k) {
+    const U v = warp_max(acc[k]);
+    if (lane == 0) red[k][warp] = v;
+  }
+  __syncthreads();
+  if (threadIdx.x < 2 * dim) {
+    U v = 0;
+    for (int w = 0; w < 8; ++w) v = max(v, red[threadIdx.x][w]);
+    atomicMax(&ctl->mm[threadIdx.x], (unsigned long long)v);
+  }
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) last = (atomicAdd(&ctl->sample_done, 1u) == gridDim.x - 1);
+  __syncthreads();
+  if (last && threadIdx.x == 0) {
+    __threadfence();
+    T mm[6];
+    for (uint32_t d = 0; d < 3; ++d) {
+      if (d < dim) {
+        const U mi = (U)(~(U)((volatile unsigned long long *)ctl->mm)[2 * d]);
+        const U ma = (U)((volatile unsigned long long *)ctl->mm)[2 * d + 1];
+        mm[d] = from_ord(mi);
+        mm[3 + d] = from_ord(ma);
+      } else {
+        mm[d] = 0;
+        mm[3 + d] = 0;
+      }
+    }
+    seg_decide(mm, dim, seg_in, rel_mode, rel_eb, eb, safe31, ctl);
+  }
+}
+
+// findMinimumValues<T> + convertRelEb<T> on the device.  The host scan starts
+// from float limits (include/utils.cuh:48-53) and ignores NaNs; 2D data has
+// z == 0 (utils.cuh:141).
+template <typename T>
+__global__ void __launch_bounds__(256) rel_to_abs_kernel(const T *__restrict__ x, const T *__restrict__ y,
+                                                         const T *__restrict__ z, uint64_t n, uint32_t dim,
+                                                         T rel, Control *ctl) {
+  using U = typename TT<T>::U;
+  __shared__ U red[6][8];
+  __shared__ int last;
+  U acc[6];
+  // min starts at FLT_MAX and max at -FLT_MAX, as on the host
+  for (int d = 0; d < 3; ++d) {
+    acc[2 * d] = (U)~ord_of((T)FLT_MAX);
+    acc[2 * d + 1] = ord_of((T)(-FLT_MAX));
+  }
+  const T *X[3] = {x, y, z};
+  const unsigned long long step = (unsigned long long)gridDim.x * blockDim.x;
+  for (unsigned long long i = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += step)
+    for (uint32_t d = 0; d < dim; ++d) fold_minmax<T>(X[d][i], acc[2 * d], acc[2 * d + 1]);
+  if (dim == 2) fold_minmax<T>((T)0, acc[4], acc[5]);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int k = 0; k < 6; ++k) {
+    const U v = warp_max(acc[k]);
+    if (lane == 0) red[k][warp] = v;
+  }
+  __syncthreads();
+  if (threadIdx.x < 6) {
+    U v = 0;
+    for (int w = 0; w < 8; ++w) v = max(v, red[threadIdx.x][w]);
+    atomicMax(&ctl->mm[threadIdx.x], (unsigned long long)v);
+  }
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) last = (atomicAdd(&ctl->sample_done, 1u) == gridDim.x - 1);
+  __syncthreads();
+  if (last && threadIdx.x == 0) {
+    __threadfence();
+    T mn[3], mx[3];
+    for (int d = 0; d < 3; ++d) {
+      mn[d] = from_ord((U)~(U)((volatile unsigned long long *)ctl->mm)[2 * d]);
+      mx[d] = from_ord((U)((volatile unsigned long long *)ctl->mm)[2 * d + 1]);
+      ctl->out_mm[d] = (double)mn[d];
+      ctl->out_mm[3 + d] = (double)mx[d];
+    }
+    T r;
+    if (sizeof(T) == 4) {
+      const float xr = __fsub_rn((float)mx[0], (float)mn[0]), yr = __fsub_rn((float)mx[1], (float)mn[1]);
+      const float zr = __fsub_rn((float)mx[2], (float)mn[2]);
+      r = (T)__fmul_rn(fmaxf(fmaxf(xr, yr), zr), (float)rel);
+    } else {
+      const double xr = __dsub_rn((double)mx[0], (double)mn[0]), yr = __dsub_rn((double)mx[1], (double)mn[1]);
+      const double zr = __dsub_rn((double)mx[2], (double)mn[2]);
+      r = (T)__dmul_rn(fmax(fmax(xr, yr), zr), (double)rel);
+    }
+    ctl->out_eb = (double)r;
+  }
+}
+
+// ===========================================================================
+// Compress.
+// ===========================================================================
+template <typename T>
+struct CArgs {
+  const T *x, *y, *z;
+  uint8_t *out;
+  unsigned long long out_cap;
+  Control *ctl;
+  unsigned long long *look;  // one look-back word per chunk
+  unsigned long long n, G;
+  T eb;
+  uint32_t dim;
+  int vec_ok;  // x, y, z all 16-byte aligned
+};
+
+template <typename T>
+struct __align__(16) CSmem {
+  uint32_t hist[kBuckets + 16];          // bucket counts -> starts; later run starts
+  unsigned long long tmp[kChunk];        // composites; later delta words [0,1024) + count words [1024,2048)
+  uint32_t sortedK[kChunk];
+  uint32_t sortedRel[kChunk];            // swizzled
+  uint32_t stage[kStageBytes / 4 + 4];   // payload staging
+  typename TT<T>::U wmm[6][kWarps];      // per-warp ordered min/max
+  uint32_t wk[3][kWarps];                // per-warp key min / key max / rel max
+  uint32_t ws1[kWarps], ws2[kWarps];     // per-warp scan totals / maxima
+  uint32_t ws3[kWarps], ws4[kWarps], ws5[kWarps];
+  uint32_t fb[kWarps][2];                // fallback sort scan totals
+  T mm[6];
+  unsigned long long bn[2];
+  unsigned long long excl;
+  uint32_t chunk;
+};
+
+constexpr unsigned long long kFlagAgg = 1ull << 62, kFlagInc = 2ull << 62, kValMask = (1ull << 62) - 1;
+
+// Decoupled look-back over the chunk sizes (warp-collective; warp 0).
+// Returns false when a bounded wait gave up or another CTA aborted.
+__device__ bool lookback(unsigned long long *look, unsigned long long c, unsigned long long agg, Control *ctl,
+                         unsigned long long &excl_out) {
+  const int lane = threadIdx.x & 31;
+  if (c == 0) {
+    if (lane == 0) st_relaxed(&look[0], kFlagInc | agg);
+    excl_out = 0;
+    return true;
+  }
+  if (lane == 0) st_relaxed(&look[c], kFlagAgg | agg);
+  unsigned long long excl = 0;
+  long long top = (long long)c - 1;
+  uint32_t spins = 0, backoff = 32;
+  while (true) {
+    const long long idx = top - lane;
+    const unsigned long long v = idx >= 0 ? ld_relaxed(&look[idx]) : kFlagInc;
+    const uint32_t fl = (uint32_t)(v >> 62);
+    const uint32_t mInc = __ballot_sync(0xFFFFFFFFu, fl == 2u);
+    const uint32_t mNone = __ballot_sync(0xFFFFFFFFu, fl == 0u);
+    const uint32_t need = mInc ? (((mInc & (0u - mInc)) << 1) - 1u) : 0xFFFFFFFFu;
+    if (mNone & need) {
+      if (++spins > kSpinLimit || ld_volatile(&ctl->abort)) {
+        if (lane == 0) {
+          atomicExch(&ctl->abort, 1u);
+          set_status(ctl, kETIMEOUT);
+        }
+        return false;
+      }
+      __nanosleep(backoff);
+      backoff = min(backoff * 2, 1024u);
+      continue;
+    }
+    unsigned long long add = ((need >> lane) & 1u) ? (v & kValMask) : 0ull;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) add += __shfl_xor_sync(0xFFFFFFFFu, add, o);
+    excl += add;
+    if (mInc) break;
+    top -= 32;
+  }
+  if (lane == 0) st_relaxed(&look[c], kFlagInc | (excl + agg));
+  excl_out = excl;
+  return true;
+}
+
+// Stable LSD radix fallback (2-bit digits) for chunks whose ranking buckets
+// are too skewed.  Elements enter in the reference's sort input order (rank
+// r = (p%32)*32 + p/32, src/cudaWarpCompress.cu:103-118, 212-218); invalid
+// tail slots carry key 2^kb so they sort last, as UINT_MAX does there.
+template <typename T>
+__device__ void fallback_sort(CSmem<T> &s, const uint32_t (&key)[4], const uint32_t (&rel)[4],
+                              const uint32_t (&r)[4], uint32_t nvalid, uint32_t kmin, uint32_t kmax) {
+  uint32_t *keyR = reinterpret_cast<uint32_t *>(s.tmp);
+  uint32_t *relR = keyR + kChunk;
+  const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+  const uint32_t kb = bitlen(kmax - kmin);
+  const uint32_t inv_key = 1u << kb;  // kb <= 31
+  // every slot of the chunk gets an entry: valid points by their rank, the
+  // tail ranks (points p >= nvalid) as invalid
+#pragma unroll
+  for (int e = 0; e < 4; ++e) {
+    const uint32_t p = 4 * t + e;
+    const bool v = p < nvalid;
+    keyR[r[e]] = v ? key[e] - kmin : inv_key;
+    relR[r[e]] = v ? rel[e] : 0xFFFFFFFFu;
+  }
+  __syncthreads();
+  const uint32_t nbits = kb + (nvalid < (uint32_t)kChunk ? 1u : 0u);
+  for (uint32_t bit = 0; bit < nbits; bit += 2) {
+    uint32_t kk[4], rr[4], d[4], lo[4];
+    uint32_t c4 = 0;  // four 8-bit local counters
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+      kk[e] = keyR[4 * t + e];
+      rr[e] = relR[4 * t + e];
+      d[e] = (kk[e] >> bit) & 3u;
+      lo[e] = (c4 >> (8 * d[e])) & 0xFFu;
+      c4 += 1u << (8 * d[e]);
+    }
+    uint32_t p0 = (c4 & 0xFFu) | (((c4 >> 8) & 0xFFu) << 16);
+    uint32_t p1 = ((c4 >> 16) & 0xFFu) | (((c4 >> 24) & 0xFFu) << 16);
+    const uint32_t q0 = p0, q1 = p1;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t v0 = __shfl_up_sync(0xFFFFFFFFu, p0, o), v1 = __shfl_up_sync(0xFFFFFFFFu, p1, o);
+      if (lane >= o) { p0 += v0; p1 += v1; }
+    }
+    if (lane == 31) { s.fb[warp][0] = p0; s.fb[warp][1] = p1; }
+    __syncthreads();
+    uint32_t w0 = 0, w1 = 0, t0 = 0, t1 = 0;
+#pragma unroll
+    for (int w = 0; w < kWarps; ++w) {
+      const uint32_t a0 = s.fb[w][0], a1 = s.fb[w][1];
+      if (w < warp) { w0 += a0; w1 += a1; }
+      t0 += a0;
+      t1 += a1;
+    }
+    const uint32_t e0 = w0 + p0 - q0, e1 = w1 + p1 - q1;  // exclusive, packed
+    const uint32_t before[4] = {e0 & 0xFFFFu, e0 >> 16, e1 & 0xFFFFu, e1 >> 16};
+    const uint32_t tot0 = t0 & 0xFFFFu, tot1 = t0 >> 16, tot2 = t1 & 0xFFFFu;
+    const uint32_t start[4] = {0u, tot0, tot0 + tot1, tot0 + tot1 + tot2};
+    __syncthreads();
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+      const uint32_t pos = start[d[e]] + before[d[e]] + lo[e];
+      keyR[pos] = kk[e];
+      relR[pos] = rr[e];
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int e = 0; e < 4; ++e) {
+    const uint32_t pos = 4 * t + e;
+    if (pos < nvalid) {
+      s.sortedK[pos] = keyR[pos] + kmin;
+      s.sortedRel[swz(pos)] = relR[pos];
+    }
+  }
+}
+
+// Writes the plane words of one 32-element group into the staging buffer.
+// Byte sections (deltas, counts): plane pi occupies bytes [pi*bpp, (pi+1)*bpp)
+// of the section, MSB plane first (src/cudaWarpCompress.cu:357-408).
+__device__ __forceinline__ void put_byte_word(uint8_t *stage8, uint32_t sec_off, uint32_t bpp, uint32_t pi,
+                                              int g, uint32_t word) {
+  const uint32_t w = to_msb_bytes(word);
+  const uint32_t base = sec_off + pi * bpp + 4u * g;
+  const uint32_t room = bpp - 4u * g;  // > 0 for every group that holds elements
+#pragma unroll
+  for (int j = 0; j < 4; ++j)
+    if ((uint32_t)j < room) stage8[base + j] = (uint8_t)(w >> (8 * j));
+}
+
+template <typename T>
+__device__ void pack_unit(CSmem<T> &s, int unit, uint32_t U, uint32_t dbits, uint32_t cbits, uint32_t rbits,
+                          uint32_t dbytes, uint32_t cbytes) {
+  const uint32_t ng = (U + 31u) >> 5;
+  const uint32_t hd = dbits ? (dbits > 16 ? 2u : 1u) * ng : 0u;
+  const uint32_t hc = cbits ? (cbits > 16 ? 2u : 1u) * ng : 0u;
+  const uint32_t hr = rbits ? (rbits > 16 ? 64u : 32u) : 0u;
+  uint32_t u = (uint32_t)unit;
+  int sec;
+  uint32_t nb;
+  const uint32_t *src;
+  if (u < hd) { sec = 0; nb = dbits; src = reinterpret_cast<const uint32_t *>(s.tmp); }
+  else if ((u -= hd) < hc) { sec = 1; nb = cbits; src = reinterpret_cast<const uint32_t *>(s.tmp) + kChunk; }
+  else if ((u -= hc) < hr) { sec = 2; nb = rbits; src = s.sortedRel; }
+  else return;
+  const uint32_t groups = sec == 2 ? 32u : ng;
+  const int g = (int)(u % groups);
+  const int half = (int)(u / groups);
+  uint32_t a[32];
+  load_group(src, g, a);
+  uint32_t b0, cnt;
+  if (nb <= 8) { transpose_lo8(a); b0 = 0; cnt = nb; }
+  else if (half == 0) { transpose_lo16(a); b0 = 0; cnt = min(nb, 16u); }
+  else { transpose_hi16(a); b0 = 16; cnt = nb - 16; }
+  uint8_t *stage8 = reinterpret_cast<uint8_t *>(s.stage);
+  const uint32_t bpp = (U + 7u) >> 3;
+  const uint32_t sec_off = sec == 0 ? 0u : dbytes;
+#pragma unroll
+  for (int k = 0; k < 16; ++k) {
+    if ((uint32_t)k < cnt) {
+      const uint32_t b = b0 + k;
+      const uint32_t pi = nb - 1u - b;
+      if (sec == 2) s.stage[((dbytes + cbytes) >> 2) + pi * 32u + g] = a[k];
+      else put_byte_word(stage8, sec_off, bpp, pi, g, a[k]);
+    }
+  }
+}
+
+template <typename T, int DIM>
+__global__ void __launch_bounds__(kThreads) compress_kernel(const CArgs<T> a) {
+  using Tr = TT<T>;
+  using U = typename Tr::U;
+  constexpr bool is64 = sizeof(T) == 8;
+  __shared__ CSmem<T> s;
+  const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+  Control *ctl = a.ctl;
+  if (ld_volatile(reinterpret_cast<const uint32_t *>(&ctl->status)) != 0) return;
+  const uint32_t seg = ctl->seg;
+  const uint32_t sh = (uint32_t)__ffs((int)seg) - 1u, msk = seg - 1u;
+  const T eb = a.eb;
+  const T inv = is64 ? (T)__ddiv_rn(1.0, __dmul_rn(2.0, (double)eb)) : (T)__fdiv_rn(1.0f, __fmul_rn(2.0f, (float)eb));
+  constexpr uint32_t dim = DIM;
+  const unsigned long long G = a.G, n = a.n;
+  const unsigned long long pay_base = Tr::hdr + 8ull * G + (unsigned long long)Tr::meta * G;
+  const T *const X[3] = {a.x, a.y, a.z};
+
+  for (;;) {
+    if (t == 0) s.chunk = ld_volatile(&ctl->abort) ? 0xFFFFFFFFu : atomicAdd(&ctl->chunk_ctr, 1u);
+    __syncthreads();  // B0
+    const unsigned long long c = s.chunk;
+    if (c >= G) break;
+    const unsigned long long base = c * kChunk;
+    const uint32_t nvalid = (uint32_t)min((unsigned long long)kChunk, n - base);
+
+    // ---- load, chunk min/max (:104-139) ----
+    T v[3][4] = {};
+    if (nvalid == (uint32_t)kChunk && a.vec_ok) {
+#pragma unroll
+      for (int d = 0; d < DIM; ++d) {
+        if (!is64) {
+          const float4 q = reinterpret_cast<const float4 *>(X[d] + base)[t];
+          v[d][0] = (T)q.x; v[d][1] = (T)q.y; v[d][2] = (T)q.z; v[d][3] = (T)q.w;
+        } else {
+          const double2 q0 = reinterpret_cast<const double2 *>(X[d] + base)[2 * t];
+          const double2 q1 = reinterpret_cast<const double2 *>(X[d] + base)[2 * t + 1];
+          v[d][0] = (T)q0.x; v[d][1] = (T)q0.y; v[d][2] = (T)q1.x; v[d][3] = (T)q1.y;
+        }
+      }
+    } else {
+#pragma unroll
+      for (int d = 0; d < DIM; ++d)
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+          const uint32_t p = 4 * t + e;
+          v[d][e] = p < nvalid ? X[d][base + p] : (T)0;
+        }
+    }
+    {
+      const T lim = is64 ? (T)DBL_MAX : (T)FLT_MAX;
+      U mn_inv[3], mx[3];
+#pragma unroll
+      for (int d = 0; d < 3; ++d) { mn_inv[d] = (U)~ord_of(lim); mx[d] = ord_of((T)-lim); }
+#pragma unroll
+      for (int d = 0; d < DIM; ++d)
+#pragma unroll
+        for (int e = 0; e < 4; ++e)
+          if (4u * t + e < nvalid) fold_minmax<T>(v[d][e], mn_inv[d], mx[d]);
+#pragma unroll
+      for (int d = 0; d < DIM; ++d) {
+        const U a0 = warp_max(mn_inv[d]), a1 = warp_max(mx[d]);
+        if (lane == 0) { s.wmm[2 * d][warp] = a0; s.wmm[2 * d + 1][warp] = a1; }
+      }
+    }
+    __syncthreads();  // B1
+    if (t < 3) {
+      if ((uint32_t)t < dim) {
+        U a0 = 0, a1 = 0;
+#pragma unroll
+        for (int w = 0; w < kWarps; ++w) { a0 = max(a0, s.wmm[2 * t][w]); a1 = max(a1, s.wmm[2 * t + 1][w]); }
+        const T mn = from_ord((U)~a0), mxv = from_ord(a1);
+        s.mm[t] = mn;
+        s.mm[3 + t] = mxv;
+        const T range = is64 ? (T)__dsub_rn((double)mxv, (double)mn) : (T)__fsub_rn((float)mxv, (float)mn);
+        if (t == 0) s.bn[0] = block_num(range, seg, eb, is64 && dim == 2);
+        if (t == 1) s.bn[1] = block_num(range, seg, eb, false);
+      } else {
+        s.mm[2] = (T)0;  // 2D meta carries z = 0 (:518, :521)
+        s.mm[5] = (T)0;
+      }
+    }
+    for (int i = t; i < kBuckets; i += kThreads) s.hist[i] = 0;
+    __syncthreads();  // B2
+
+    // ---- quantize, block id, relative position (:141-205) ----
+    uint32_t key[4], rel[4], r[4];
+    uint32_t kmin = 0xFFFFFFFFu, kmax = 0u, rmax = 0u;
+    {
+      T nmn[3];
+#pragma unroll
+      for (int d = 0; d < 3; ++d)
+        nmn[d] = is64 ? (T)__dmul_rn(-(double)s.mm[d], (double)inv) : (T)__fmul_rn(-(float)s.mm[d], (float)inv);
+      const unsigned long long bnx = s.bn[0], bny = s.bn[1];
+#pragma unroll
+      for (int e = 0; e < 4; ++e) {
+        const uint32_t p = 4 * t + e;
+        r[e] = (p & 31u) * 32u + (p >> 5);
+        if (!is64) {
+          const uint32_t bx = (uint32_t)bnx, bxy = (uint32_t)bnx * (uint32_t)bny;
+          const uint32_t qx = __float2uint_rz(__fmaf_rn((float)v[0][e], (float)inv, (float)nmn[0]));
+          const uint32_t qy = __float2uint_rz(__fmaf_rn((float)v[1][e], (float)inv, (float)nmn[1]));
+          if (dim == 3) {
+            const uint32_t qz = __float2uint_rz(__fmaf_rn((float)v[2][e], (float)inv, (float)nmn[2]));
+            key[e] = ((qx >> sh) + (qy >> sh) * bx + (qz >> sh) * bxy) & 0x7FFFFFFFu;
+            rel[e] = ((qx & msk) + (qy & msk) * seg + (qz & msk) * (seg * seg)) & 0x7FFFFFFFu;
+          } else {
+            key[e] = ((qx >> sh) + (qy >> sh) * bx) & 0x7FFFFFFFu;
+            rel[e] = ((qx & msk) + (qy & msk) * seg) & 0x7FFFFFFFu;
+          }
+        } else {
+          // All arithmetic below is mod 2^32 of the reference's u64 expression,
+          // which is exact because the result is masked to 31 bits.
+          const unsigned long long qx = __double2ull_rz(__fma_rn((double)v[0][e], (double)inv, (double)nmn[0]));
+          const unsigned long long qy = __double2ull_rz(__fma_rn((double)v[1][e], (double)inv, (double)nmn[1]));
+          const uint32_t bx = (uint32_t)bnx;
+          if (dim == 3) {
+            const unsigned long long qz = __double2ull_rz(__fma_rn((double)v[2][e], (double)inv, (double)nmn[2]));
+            const uint32_t bxy = (uint32_t)(bnx * bny);
+            key[e] = ((uint32_t)(qx >> sh) + (uint32_t)(qy >> sh) * bx + (uint32_t)(qz >> sh) * bxy) & 0x7FFFFFFFu;
+            rel[e] = ((uint32_t)(qx & msk) + (uint32_t)(qy & msk) * seg + (uint32_t)(qz & msk) * seg * seg) &
+                     0x7FFFFFFFu;
+          } else {
+            key[e] = ((uint32_t)(qx >> sh) + (uint32_t)(qy >> sh) * bx) & 0x7FFFFFFFu;
+            rel[e] = ((uint32_t)(qx & msk) + (uint32_t)(qy & msk) * seg) & 0x7FFFFFFFu;
+          }
+        }
+        if (p < nvalid) {
+          kmin = min(kmin, key[e]);
+          kmax = max(kmax, key[e]);
+          rmax = max(rmax, rel[e]);
+        }
+      }
+      if (t == 0) {
+        // block-id overflow check on the chunk's largest quantized corner
+        unsigned long long qm[3] = {0, 0, 0};
+#pragma unroll
+        for (int d = 0; d < DIM; ++d)
+          qm[d] = is64 ? __double2ull_rz(__fma_rn((double)s.mm[3 + d], (double)inv, (double)nmn[d]))
+                       : (unsigned long long)__float2uint_rz(__fmaf_rn((float)s.mm[3 + d], (float)inv, (float)nmn[d]));
+        const unsigned long long bound = (qm[0] >> sh) + (qm[1] >> sh) * bnx + (dim == 3 ? (qm[2] >> sh) * bnx * bny : 0ull);
+        if (bound > 0x7FFFFFFFull) ctl->id_overflow = 1u;
+      }
+    }
+    {
+      const uint32_t a0 = warp_min(kmin), a1 = warp_max(kmax), a2 = warp_max(rmax);
+      if (lane == 0) { s.wk[0][warp] = a0; s.wk[1][warp] = a1; s.wk[2][warp] = a2; }
+    }
+    __syncthreads();  // B3
+    kmin = 0xFFFFFFFFu; kmax = 0; rmax = 0;
+#pragma unroll
+    for (int w = 0; w < kWarps; ++w) {
+      kmin = min(kmin, s.wk[0][w]);
+      kmax = max(kmax, s.wk[1][w]);
+      rmax = max(rmax, s.wk[2][w]);
+    }
+    const uint32_t rbits = max(bitlen(rmax), nvalid < (uint32_t)kChunk ? 1u : 0u);  // :200-201
+
+    // ---- ranking: bucket the unique composite (block id, rank) ----
+    const unsigned long long cmax = ((unsigned long long)(kmax - kmin) << 10) | 1023ull;
+    const uint32_t shb = (uint32_t)max(0, (int)bitlen64(cmax) - 10);
+    unsigned long long C[4];
+    uint32_t bk[4], slot[4];
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+      C[e] = ((unsigned long long)(key[e] - kmin) << 10) | r[e];
+      bk[e] = (uint32_t)(C[e] >> shb);
+      if (4u * t + e < nvalid) slot[e] = atomicAdd(&s.hist[bk[e]], 1u);
+    }
+    __syncthreads();  // B4
+    uint32_t gmaxc;
+    {
+      const uint4 h = reinterpret_cast<const uint4 *>(s.hist)[t];
+      const uint32_t s0 = h.x, s1 = s0 + h.y, s2 = s1 + h.z, s3 = s2 + h.w;
+      uint32_t inc = s3;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t q = __shfl_up_sync(0xFFFFFFFFu, inc, o);
+        if (lane >= o) inc += q;
+      }
+      const uint32_t mc = warp_max(max(max(h.x, h.y), max(h.z, h.w)));
+      if (lane == 31) { s.ws1[warp] = inc; s.ws2[warp] = mc; }
+      __syncthreads();  // B5
+      uint32_t pre = 0;
+      gmaxc = 0;
+#pragma unroll
+      for (int w = 0; w < kWarps; ++w) {
+        if (w < warp) pre += s.ws1[w];
+        gmaxc = max(gmaxc, s.ws2[w]);
+      }
+      const uint32_t ex = pre + inc - s3;
+      reinterpret_cast<uint4 *>(s.hist)[t] = make_uint4(ex, ex + s0, ex + s1, ex + s2);
+      if (t == kThreads - 1) s.hist[kBuckets] = ex + s3;
+    }
+    __syncthreads();  // B6
+    if (gmaxc <= (uint32_t)kBucketLimit) {
+#pragma unroll
+      for (int e = 0; e < 4; ++e)
+        if (4u * t + e < nvalid) s.tmp[s.hist[bk[e]] + slot[e]] = C[e];
+      __syncthreads();  // B7
+#pragma unroll
+      for (int e = 0; e < 4; ++e) {
+        if (4u * t + e < nvalid) {
+          const uint32_t st = s.hist[bk[e]], en = s.hist[bk[e] + 1];
+          uint32_t rank = 0;
+          for (uint32_t j = st; j < en; ++j) rank += (s.tmp[j] < C[e]) ? 1u : 0u;
+          const uint32_t pos = st + rank;
+          s.sortedK[pos] = key[e];
+          s.sortedRel[swz(pos)] = rel[e];
+        }
+      }
+    } else {
+      fallback_sort<T>(s, key, rel, r, nvalid, kmin, kmax);
+    }
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+      const uint32_t pos = 4 * t + e;
+      if (pos >= nvalid) s.sortedRel[swz(pos)] = 0xFFFFFFFFu;  // invalid slots (:197)
+    }
+    __syncthreads();  // B8
+
+    // ---- runs: unique ids, deltas, counts (:222-311) ----
+    uint32_t* const runStart = s.hist;
+    uint32_t* const deltaA = reinterpret_cast<uint32_t *>(s.tmp);
+    uint32_t* const countA = deltaA + kChunk;
+    uint32_t Ucnt, dbits, cbits;
+    {
+      const uint4 k4 = reinterpret_cast<const uint4 *>(s.sortedK)[t];
+      const uint32_t kk[4] = {k4.x, k4.y, k4.z, k4.w};
+      const uint32_t prev = t > 0 ? s.sortedK[4 * t - 1] : 0u;
+      uint32_t f = 0, dm = 0, cnt = 0;
+      uint32_t dl[4];
+#pragma unroll
+      for (int e = 0; e < 4; ++e) {
+        const uint32_t pos = 4 * t + e;
+        const uint32_t pk = e ? kk[e - 1] : prev;
+        const bool fl = pos < nvalid && (pos == 0 || kk[e] != pk);
+        dl[e] = pos == 0 ? 0u : kk[e] - pk;
+        if (fl) { f |= 1u << e; ++cnt; dm = max(dm, bitlen(dl[e])); }
+      }
+      uint32_t inc = cnt;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t q = __shfl_up_sync(0xFFFFFFFFu, inc, o);
+        if (lane >= o) inc += q;
+      }
+      const uint32_t wd = warp_max(dm);
+      if (lane == 31) { s.ws3[warp] = inc; s.ws4[warp] = wd; }
+      __syncthreads();  // B9
+      uint32_t pre = 0;
+      Ucnt = 0;
+      dbits = 0;
+#pragma unroll
+      for (int w = 0; w < kWarps; ++w) {
+        if (w < warp) pre += s.ws3[w];
+        Ucnt += s.ws3[w];
+        dbits = max(dbits, s.ws4[w]);
+      }
+      uint32_t u = pre + inc - cnt;
+#pragma unroll
+      for (int e = 0; e < 4; ++e)
+        if (f & (1u << e)) {
+          runStart[u] = 4 * t + e;
+          deltaA[swz(u)] = dl[e];
+          ++u;
+        }
+      if (t == 0) runStart[Ucnt] = nvalid;
+    }
+    __syncthreads();  // B10
+    {
+      uint32_t cm = 0;
+#pragma unroll
+      for (int e = 0; e < 4; ++e) {
+        const uint32_t u = 4 * t + e;
+        if (u < Ucnt) {
+          const uint32_t cv = runStart[u + 1] - runStart[u];
+          countA[swz(u)] = cv;
+          cm = max(cm, bitlen(cv));
+        } else {
+          countA[swz(u)] = 0u;
+          deltaA[swz(u)] = 0u;
+        }
+      }
+      cm = warp_max(cm);
+      if (lane == 0) s.ws5[warp] = cm;
+    }
+    __syncthreads();  // B11
+    cbits = 0;
+#pragma unroll
+    for (int w = 0; w < kWarps; ++w) cbits = max(cbits, s.ws5[w]);
+
+    const uint32_t dbytes = section_bytes(Ucnt, dbits, Tr::pad);
+    const uint32_t cbytes = section_bytes(Ucnt, cbits, Tr::pad);
+    const uint32_t rbytes = rel_section_bytes(rbits, Tr::pad);
+    const uint32_t payload = dbytes + cbytes + rbytes;
+
+    // ---- place the chunk (look-back) while the other warps pack planes ----
+    if (warp == 0) {
+      unsigned long long excl = 0;
+      const bool ok = lookback(a.look, c, payload, ctl, excl);
+      if (lane == 0) s.excl = ok ? excl : ~0ull;
+      if (ok) {
+        // offset table entry (:1679) and meta record (:332-344)
+        if (lane == 0) reinterpret_cast<unsigned long long *>(a.out + Tr::hdr)[c] = excl;
+        uint8_t *meta = a.out + Tr::hdr + 8ull * G + (unsigned long long)Tr::meta * c;
+        if (!is64) {
+          uint32_t *m32 = reinterpret_cast<uint32_t *>(meta);
+          if (lane < 6) m32[lane] = __float_as_uint((float)s.mm[lane]);
+          if (lane == 6) m32[6] = s.sortedK[0];
+          if (lane == 7) m32[7] = dbits | (cbits << 16);
+          if (lane == 8) m32[8] = rbits | (Ucnt << 16);
+        } else {
+          unsigned long long *m64 = reinterpret_cast<unsigned long long *>(meta);
+          if (lane < 6) m64[lane] = (unsigned long long)__double_as_longlong((double)s.mm[lane]);
+          if (lane == 6) m64[6] = s.sortedK[0];
+          if (lane == 7)
+            m64[7] = (unsigned long long)dbits | ((unsigned long long)cbits << 16) |
+                     ((unsigned long long)rbits << 32) | ((unsigned long long)Ucnt << 48);
+        }
+        if (c == 0) {
+          // header (:1674-1678; Double :1672-1680)
+          uint32_t *h = reinterpret_cast<uint32_t *>(a.out);
+          if (lane == 0) h[0] = dim;
+          if (lane == 1) h[1] = (uint32_t)n;
+          if (lane == 2) h[2] = (uint32_t)(n >> 32);
+          if (lane == 3) h[3] = Tr::bits;
+          if (!is64) {
+            if (lane == 4) h[4] = __float_as_uint((float)eb);
+            if (lane == 5) h[5] = seg;
+          } else {
+            if (lane == 4) reinterpret_cast<unsigned long long *>(a.out)[2] = (unsigned long long)__double_as_longlong((double)eb);
+            if (lane == 6) h[6] = seg;
+            if (lane == 7) h[7] = 32u;
+          }
+        }
+        if (c == G - 1 && lane == 0) ctl->stream_bytes = pay_base + excl + payload;
+      }
+    } else {
+      const int unit = t - 32;
+      pack_unit<T>(s, unit, Ucnt, dbits, cbits, rbits, dbytes, cbytes);
+      if (t == kThreads - 1) {
+        // section padding is zero (the reference leaves it unwritten)
+        uint8_t *stage8 = reinterpret_cast<uint8_t *>(s.stage);
+        const uint32_t bpp = (Ucnt + 7u) >> 3;
+        for (uint32_t i = dbits * bpp; i < dbytes; ++i) stage8[i] = 0;
+        for (uint32_t i = dbytes + cbits * bpp; i < dbytes + cbytes; ++i) stage8[i] = 0;
+      }
+    }
+    __syncthreads();  // B12
+    const unsigned long long excl = s.excl;
+    if (excl != ~0ull) {
+      if (pay_base + excl + payload > a.out_cap) {
+        if (t == 0) set_status(ctl, kENOSPACE);
+      } else {
+        uint32_t *dst = reinterpret_cast<uint32_t *>(a.out + pay_base + excl);
+        for (uint32_t w = t; w < payload / 4u; w += kThreads) dst[w] = s.stage[w];
+      }
+    }
+  }
+}
+
+// ===========================================================================
+// Decompress.
+// ===========================================================================
+template <typename T>
+struct DArgs {
+  const uint8_t *s;
+  unsigned long long bytes;
+  T *x, *y, *z;
+  unsigned long long cap;
+  Control *ctl;
+  int vec_ok;
+};
+
+template <typename T>
+struct __align__(16) DSmem {
+  uint32_t stage[kStageBytes / 4 + 8];
+  uint32_t dv[kChunk];      // deltas (swizzled) -> ids (low words)
+  uint32_t dvh[kChunk];     // ids high words (float64 streams)
+  uint32_t cv[kChunk];      // counts (swizzled) -> run starts
+  uint32_t rv[kChunk];      // relative positions (swizzled)
+  uint32_t runAt[kChunk];   // run index at each run start
+  uint32_t ws[4][kWarps];
+  T mm[6];
+  unsigned long long first, off;
+  FastDiv fx, fy, fxy;
+  unsigned long long bnx, bny;
+  uint32_t U, dbits, cbits, rbits, dbytes, cbytes, payload, ok, slow;
+  uint32_t chunk;
+};
+
+template <typename T, int DIM>
+__global__ void __launch_bounds__(kThreads) decompress_kernel(const DArgs<T> a) {
+  using Tr = TT<T>;
+  constexpr bool is64 = sizeof(T) == 8;
+  __shared__ DSmem<T> s;
+  const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+  Control *ctl = a.ctl;
+  // ---- header (:1801-1828) ----
+  if (a.bytes < Tr::hdr) { if (t == 0) set_status(ctl, kESTREAM); return; }
+  const uint32_t dim = *reinterpret_cast<const uint32_t *>(a.s);
+  unsigned long long n;
+  memcpy(&n, a.s + 4, 8);
+  const uint32_t bits = *reinterpret_cast<const uint32_t *>(a.s + 12);
+  T eb;
+  memcpy(&eb, a.s + 16, sizeof(T));
+  const uint32_t seg = *reinterpret_cast<const uint32_t *>(a.s + 16 + sizeof(T));
+  const unsigned long long G = (n + kChunk - 1) / kChunk;
+  if (bits != Tr::bits || dim != (uint32_t)DIM || n == 0 || seg == 0 ||
+      G > (a.bytes - Tr::hdr) / (8ull + Tr::meta)) {
+    if (t == 0) set_status(ctl, kESTREAM);
+    return;
+  }
+  if (n > a.cap) { if (t == 0) set_status(ctl, kENOSPACE); return; }
+  const unsigned long long pay_base = Tr::hdr + 8ull * G + (unsigned long long)Tr::meta * G;
+  const uint32_t sh = (uint32_t)__ffs((int)seg) - 1u, msk = seg - 1u;
+  T *const Y[3] = {a.x, a.y, a.z};
+
+  for (;;) {
+    if (t == 0) s.chunk = ld_volatile(&ctl->abort) ? 0xFFFFFFFFu : atomicAdd(&ctl->chunk_ctr, 1u);
+    __syncthreads();  // B0
+    const unsigned long long c = s.chunk;
+    if (c >= G) break;
+    const unsigned long long base = c * kChunk;
+    const uint32_t nvalid = (uint32_t)min((unsigned long long)kChunk, n - base);
+    if (t == 0) {
+      const uint8_t *m = a.s + Tr::hdr + 8ull * G + (unsigned long long)Tr::meta * c;
+      T mm[6];
+      memcpy(mm, m, sizeof(mm));
+      unsigned long long first;
+      uint32_t dbits, cbits, rbits, U;
+      if (!is64) {
+        first = *reinterpret_cast<const uint32_t *>(m + 24);
+        const uint32_t w7 = *reinterpret_cast<const uint32_t *>(m + 28), w8 = *reinterpret_cast<const uint32_t *>(m + 32);
+        dbits = w7 & 0xFFFFu; cbits = w7 >> 16; rbits = w8 & 0xFFFFu; U = w8 >> 16;
+      } else {
+        first = *reinterpret_cast<const unsigned long long *>(m + 48);
+        const unsigned long long w7 = *reinterpret_cast<const unsigned long long *>(m + 56);
+        dbits = (uint32_t)(w7 & 0xFFFFu); cbits = (uint32_t)((w7 >> 16) & 0xFFFFu);
+        rbits = (uint32_t)((w7 >> 32) & 0xFFFFu); U = (uint32_t)(w7 >> 48);
+      }
+      const unsigned long long off = reinterpret_cast<const unsigned long long *>(a.s + Tr::hdr)[c];
+      const uint32_t db = section_bytes(U, dbits, Tr::pad), cb = section_bytes(U, cbits, Tr::pad);
+      const uint32_t rb = rel_section_bytes(rbits, Tr::pad);
+      const unsigned long long pl = (unsigned long long)db + cb + rb;
+      uint32_t ok = U >= 1 && U <= nvalid && dbits <= 32 && cbits <= 32 && rbits <= 32 &&
+                    (off & (Tr::pad)) == 0 &&
+                    pl <= (unsigned long long)kStageBytes && pay_base <= a.bytes && off <= a.bytes - pay_base &&
+                    pl <= a.bytes - pay_base - off;
+      for (int k = 0; k < 6; ++k) s.mm[k] = mm[k];
+      s.first = first; s.off = off;
+      s.U = U; s.dbits = dbits; s.cbits = cbits; s.rbits = rbits;
+      s.dbytes = db; s.cbytes = cb; s.payload = (uint32_t)pl; s.ok = ok;
+      // block counts (:831-837 / Double :835-838) and exact dividers
+      const T rx = is64 ? (T)__dsub_rn((double)mm[3], (double)mm[0]) : (T)__fsub_rn((float)mm[3], (float)mm[0]);
+      const T ry = is64 ? (T)__dsub_rn((double)mm[4], (double)mm[1]) : (T)__fsub_rn((float)mm[4], (float)mm[1]);
+      const unsigned long long bnx = block_num(rx, seg, eb, false), bny = block_num(ry, seg, eb, false);
+      s.bnx = bnx; s.bny = bny;
+      if (!is64) {
+        s.fx.init((uint32_t)bnx); s.fy.init((uint32_t)bny); s.fxy.init((uint32_t)bnx * (uint32_t)bny);
+        s.slow = 0;
+      } else {
+        const bool fits = (bnx >> 32) == 0 && (bny >> 32) == 0 && ((bnx * bny) >> 32) == 0;
+        s.slow = fits ? 0u : 1u;
+        s.fx.init((uint32_t)bnx); s.fy.init((uint32_t)bny); s.fxy.init((uint32_t)(bnx * bny));
+      }
+      if (!ok) set_status(ctl, kESTREAM);
+    }
+    for (int i = t; i < kChunk; i += kThreads) s.runAt[i] = 0;
+    __syncthreads();  // B1
+    if (!s.ok) continue;
+    const uint32_t U = s.U, dbits = s.dbits, cbits = s.cbits, rbits = s.rbits;
+    {
+      const uint32_t *src = reinterpret_cast<const uint32_t *>(a.s + pay_base + s.off);
+      const uint32_t nw = s.payload >> 2;
+      for (uint32_t w = t; w < nw; w += kThreads) s.stage[w] = src[w];
+      if (t < 8) s.stage[nw + t] = 0u;
+    }
+    __syncthreads();  // B2
+
+    // ---- bit planes -> values (:864-927) ----
+    {
+      const uint32_t ng = (U + 31u) >> 5;
+      // every section gets its units, also with 0 bits (values then decode as 0)
+      const uint32_t nd = ng, nc = ng, nr = 32u;
+      uint32_t u = (uint32_t)t;
+      int sec = -1;
+      if (u < nd) sec = 0;
+      else if ((u -= nd) < nc) sec = 1;
+      else if ((u -= nc) < nr) sec = 2;
+      if (sec >= 0) {
+        const int g = (int)u;
+        const uint32_t nb = sec == 0 ? dbits : (sec == 1 ? cbits : rbits);
+        uint32_t pw[32];
+        const uint8_t *stage8 = reinterpret_cast<const uint8_t *>(s.stage);
+        const uint32_t bpp = (U + 7u) >> 3;
+        const uint32_t sec_off = sec == 0 ? 0u : s.dbytes;
+        const uint32_t room = bpp - 4u * g;
+#pragma unroll
+        for (int b = 0; b < 32; ++b) {
+          uint32_t w = 0;
+          if ((uint32_t)b < nb) {
+            const uint32_t pi = nb - 1u - b;
+            if (sec == 2) {
+              w = s.stage[((s.dbytes + s.cbytes) >> 2) + pi * 32u + g];
+            } else {
+              const uint32_t at = sec_off + pi * bpp + 4u * g;
+              const uint32_t a0 = at >> 2, shf = (at & 3u) * 8u;
+              w = __funnelshift_r(s.stage[a0], s.stage[a0 + 1], shf);
+              if (room < 4u) w &= (1u << (8u * room)) - 1u;
+              w = from_msb_bytes(w);
+            }
+          }
+          pw[b] = w;
+        }
+        (void)stage8;
+        transpose32(pw);
+        store_group(sec == 0 ? s.dv : (sec == 1 ? s.cv : s.rv), g, pw);
+      }
+    }
+    __syncthreads();  // B3
+
+    // ---- ids = first + prefix of deltas; run starts = prefix of counts (:930-938) ----
+    uint32_t idl[4], idh[4];
+    bool chunk_ok;
+    {
+      uint32_t dl[4], cl[4];
+#pragma unroll
+      for (int e = 0; e < 4; ++e) {
+        const uint32_t u = 4 * t + e;
+        dl[e] = (u < U && u > 0) ? s.dv[swz(u)] : 0u;  // delta[0] is replaced by the first id
+        cl[e] = u < U ? s.cv[swz(u)] : 0u;
+      }
+      // inclusive scans: deltas (64-bit), counts (32-bit sums; 64-bit to catch overflow)
+      unsigned long long dsum = 0, csum = 0;
+      unsigned long long dinc[4], cinc[4];
+#pragma unroll
+      for (int e = 0; e < 4; ++e) { dsum += dl[e]; dinc[e] = dsum; csum += cl[e]; cinc[e] = csum; }
+      unsigned long long di = dsum, ci = csum;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const unsigned long long q0 = __shfl_up_sync(0xFFFFFFFFu, di, o), q1 = __shfl_up_sync(0xFFFFFFFFu, ci, o);
+        if (lane >= o) { di += q0; ci += q1; }
+      }
+      if (lane == 31) {
+        s.ws[0][warp] = (uint32_t)di; s.ws[1][warp] = (uint32_t)(di >> 32);
+        s.ws[2][warp] = (uint32_t)ci; s.ws[3][warp] = (uint32_t)(ci >> 32);
+      }
+      __syncthreads();  // B4
+      unsigned long long dpre = 0, cpre = 0, ctot = 0;
+#pragma unroll
+      for (int w = 0; w < kWarps; ++w) {
+        const unsigned long long dw = s.ws[0][w] | ((unsigned long long)s.ws[1][w] << 32);
+        const unsigned long long cw = s.ws[2][w] | ((unsigned long long)s.ws[3][w] << 32);
+        if (w < warp) { dpre += dw; cpre += cw; }
+        ctot += cw;
+      }
+      chunk_ok = ctot == nvalid;
+      const unsigned long long dbase = dpre + di - dsum, cbase = cpre + ci - csum;
+#pragma unroll
+      for (int e = 0; e < 4; ++e) {
+        const uint32_t u = 4 * t + e;
+        const unsigned long long id = s.first + dbase + dinc[e];
+        idl[e] = (uint32_t)id;
+        idh[e] = (uint32_t)(id >> 32);
+        if (u < U && chunk_ok) {
+          const uint32_t st = (uint32_t)(cbase + cinc[e] - cl[e]);
+          if (st < (uint32_t)kChunk) atomicMax(&s.runAt[st], u);
+        }
+      }
+    }
+    __syncthreads();  // B5
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+      const uint32_t u = 4 * t + e;
+      s.dv[u] = idl[e];
+      s.dvh[u] = idh[e];
+    }
+    // run index at every position: inclusive max-scan of the run-start marks
+    uint32_t ra[4];
+    {
+      const uint4 m4 = reinterpret_cast<const uint4 *>(s.runAt)[t];
+      ra[0] = m4.x; ra[1] = max(ra[0], m4.y); ra[2] = max(ra[1], m4.z); ra[3] = max(ra[2], m4.w);
+      uint32_t inc = ra[3];
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t q = __shfl_up_sync(0xFFFFFFFFu, inc, o);
+        if (lane >= o) inc = max(inc, q);
+      }
+      const uint32_t prevw = __shfl_up_sync(0xFFFFFFFFu, inc, 1);
+      if (lane == 31) s.ws[0][warp] = inc;
+      __syncthreads();  // B6
+      uint32_t pre = 0;
+#pragma unroll
+      for (int w = 0; w < kWarps; ++w)
+        if (w < warp) pre = max(pre, s.ws[0][w]);
+      if (lane > 0) pre = max(pre, prevw);
+#pragma unroll
+      for (int e = 0; e < 4; ++e) ra[e] = max(ra[e], pre);
+    }
+    if (!chunk_ok) {
+      if (t == 0) set_status(ctl, kESTREAM);
+      continue;
+    }
+
+    // ---- reconstruct (:971-1007): q = block*seg + rel, v = fma(2q+1, eb, min) ----
+    T out[3][4] = {};
+    const T mnx = s.mm[0], mny = s.mm[1], mnz = s.mm[2];
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+      const uint32_t pos = 4 * t + e;
+      const uint32_t run = ra[e];
+      const uint32_t rp = s.rv[swz(pos)];
+      const uint32_t idlo = s.dv[run];
+      if (!is64) {
+        const uint32_t id = idlo;
+        const uint32_t bx = s.fx.mod(id), by = s.fy.mod(s.fx.div(id));
+        const uint32_t rx = rp & msk, ry = (rp >> sh) & msk;
+        const uint32_t qx = bx * seg + rx, qy = by * seg + ry;
+        out[0][e] = (T)__fmaf_rn(__uint2float_rn((qx << 1) | 1u), (float)eb, (float)mnx);
+        out[1][e] = (T)__fmaf_rn(__uint2float_rn((qy << 1) | 1u), (float)eb, (float)mny);
+        if (DIM == 3) {
+          const uint32_t bz = s.fxy.div(id);
+          const uint32_t rz = (2u * sh >= 32u) ? 0u : (rp >> (2u * sh));
+          const uint32_t qz = bz * seg + rz;
+          out[2][e] = (T)__fmaf_rn(__uint2float_rn((qz << 1) | 1u), (float)eb, (float)mnz);
+        }
+      } else {
+        const unsigned long long id = idlo | ((unsigned long long)s.dvh[run] << 32);
+        unsigned long long bx, by, bz = 0;
+        if (!s.slow && (id >> 32) == 0) {
+          const uint32_t i32 = (uint32_t)id;
+          bx = s.fx.mod(i32);
+          by = s.fy.mod(s.fx.div(i32));
+          if (DIM == 3) bz = s.fxy.div(i32);
+        } else {
+          const unsigned long long dx = s.bnx, dy = s.bny, dxy = s.bnx * s.bny;
+          bx = dx ? id % dx : id;
+          const unsigned long long q1 = dx ? id / dx : ~0ull;
+          by = dy ? q1 % dy : q1;
+          bz = dxy ? id / dxy : ~0ull;
+        }
+        const unsigned long long r64 = rp, m64 = msk, s64 = seg;
+        const unsigned long long rx = r64 & m64, ry = (r64 >> sh) & m64, rz = r64 >> (2u * sh);
+        const unsigned long long qx = bx * s64 + rx, qy = by * s64 + ry, qz = bz * s64 + rz;
+        out[0][e] = (T)__fma_rn(__ull2double_rn((qx << 1) | 1ull), (double)eb, (double)mnx);
+        out[1][e] = (T)__fma_rn(__ull2double_rn((qy << 1) | 1ull), (double)eb, (double)mny);
+        if (DIM == 3) out[2][e] = (T)__fma_rn(__ull2double_rn((qz << 1) | 1ull), (double)eb, (double)mnz);
+      }
+    }
+    if (nvalid == (uint32_t)kChunk && a.vec_ok) {
+#pragma unroll
+      for (int d = 0; d < DIM; ++d) {
+        if (!is64) {
+          reinterpret_cast<float4 *>(Y[d] + base)[t] =
+              make_float4((float)out[d][0], (float)out[d][1], (float)out[d][2], (float)out[d][3]);
+        } else {
+          reinterpret_cast<double2 *>(Y[d] + base)[2 * t] = make_double2((double)out[d][0], (double)out[d][1]);
+          reinterpret_cast<double2 *>(Y[d] + base)[2 * t + 1] = make_double2((double)out[d][2], (double)out[d][3]);
+        }
+      }
+    } else {
+#pragma unroll
+      for (int d = 0; d < DIM; ++d)
+#pragma unroll
+        for (int e = 0; e < 4; ++e)
+          if (4u * t + e < nvalid) Y[d][base + 4 * t + e] = out[d][e];
+    }
+  }
+}
+
+}  // namespace gpzb

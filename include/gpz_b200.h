@@ -113,17 +113,17 @@ int gpz_compress(const gpz_params *params, const void *d_x, const void *d_y, con
  * reached through CompressorManager::decompressWarp (src/CompressorManager.cpp:18-22).
  *
  * d_stream: the compressed stream on the device, stream_bytes long.
- * float_bits must match the stream header (the caller reads it from its host
- * copy with gpz_parse_header, as decompressLoadParas does).  Outputs are SoA,
+ * float_bits and dim must match the stream header (the caller reads them from
+ * its host copy with gpz_parse_header, as decompressLoadParas does).  Outputs are SoA,
  * out_capacity points each; points come out in the stream's order (sorted by
  * block within each 1024-point chunk), as in the reference.  d_z is ignored
  * for 2D streams.  Header and every chunk record are validated on the device;
  * a bad chunk sets GPZ_ESTREAM and is not written. */
 int gpz_decompress_async(const void *d_stream, uint64_t stream_bytes, uint32_t float_bits,
-                         void *d_x, void *d_y, void *d_z, uint64_t out_capacity,
+                         uint32_t dim, void *d_x, void *d_y, void *d_z, uint64_t out_capacity,
                          void *d_scratch, uint64_t scratch_bytes, void *stream);
 
-int gpz_decompress(const void *d_stream, uint64_t stream_bytes, uint32_t float_bits,
+int gpz_decompress(const void *d_stream, uint64_t stream_bytes, uint32_t float_bits, uint32_t dim,
                    void *d_x, void *d_y, void *d_z, uint64_t out_capacity, void *d_scratch,
                    uint64_t scratch_bytes, gpz_result *result, void *stream);
 
