@@ -18,10 +18,18 @@ constexpr int kThreads = 256;       // threads per CTA
 constexpr int kWarps = kThreads / 32;
 constexpr int kEPT = kChunk / kThreads;   // points per thread (4)
 constexpr int kBuckets = 1024;      // ranking buckets per chunk
-constexpr int kBucketLimit = 64;    // larger buckets switch the chunk to the radix fallback
+constexpr int kSmallBucket = 16;    // larger ranking buckets are sorted by a warp
 constexpr int kStageBytes = 9472;   // >= max payload: 31*128 + 11*128 + 31*128 + padding
 constexpr uint32_t kSpinLimit = 1u << 22;  // bounded waits in the look-back scan
 constexpr int kCtlBytes = 256;      // control block at the head of scratch
+#ifndef GPZ_COMPRESS_MIN_BLOCKS
+#define GPZ_COMPRESS_MIN_BLOCKS 4
+#endif
+#ifndef GPZ_DECOMPRESS_MIN_BLOCKS
+#define GPZ_DECOMPRESS_MIN_BLOCKS 4
+#endif
+constexpr int kCompressMinBlocks = GPZ_COMPRESS_MIN_BLOCKS;      // resident CTAs per SM the
+constexpr int kDecompressMinBlocks = GPZ_DECOMPRESS_MIN_BLOCKS;  // register budget is sized for
 
 // Error codes (same values as include/gpz_b200.h).
 constexpr int kOK = 0, kEINVAL = 1, kESEG = 2, kESTREAM = 3, kENOSPACE = 4, kETIMEOUT = 6;

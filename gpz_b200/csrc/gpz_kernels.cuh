@@ -250,12 +250,17 @@ struct __align__(16) CSmem {
   unsigned long long tmp[kChunk];        // composites; later delta words [0,1024) + count words [1024,2048)
   uint32_t sortedK[kChunk];
   uint32_t sortedRel[kChunk];            // swizzled
-  uint32_t stage[kStageBytes / 4 + 4];   // payload staging
+  uint32_t relR[kChunk];                 // relative position by sort rank r
+  uint16_t big[kBuckets];                // buckets ranked by a warp sort
+  uint32_t nbig;
+  uint32_t stage[2][kStageBytes / 4 + 4];  // payload staging, two chunks in flight
+  uint32_t pmeta[2][16];                 // meta record of the staged chunk
+  unsigned long long pchunk[2];          // chunk id of the staged chunk (~0 = none)
+  uint32_t ppay[2];                      // payload bytes of the staged chunk
   typename TT<T>::U wmm[6][kWarps];      // per-warp ordered min/max
   uint32_t wk[3][kWarps];                // per-warp key min / key max / rel max
-  uint32_t ws1[kWarps], ws2[kWarps];     // per-warp scan totals / maxima
+  uint32_t ws1[kWarps];                  // per-warp scan totals / maxima
   uint32_t ws3[kWarps], ws4[kWarps], ws5[kWarps];
-  uint32_t fb[kWarps][2];                // fallback sort scan totals
   T mm[6];
   unsigned long long bn[2];
   unsigned long long excl;
@@ -264,17 +269,25 @@ struct __align__(16) CSmem {
 
 constexpr unsigned long long kFlagAgg = 1ull << 62, kFlagInc = 2ull << 62, kValMask = (1ull << 62) - 1;
 
-// Decoupled look-back over the chunk sizes (warp-collective; warp 0).
-// Returns false when a bounded wait gave up or another CTA aborted.
-__device__ bool lookback(unsigned long long *look, unsigned long long c, unsigned long long agg, Control *ctl,
-                         unsigned long long &excl_out) {
+// Decoupled look-back over the chunk sizes.  A chunk publishes its own
+// payload size (aggregate) as soon as it knows it; placing it later
+// (resolve_prefix, one CTA iteration afterwards) sums the aggregates of its
+// predecessors back to the nearest published inclusive prefix, then
+// publishes its own inclusive prefix.
+__device__ __forceinline__ void publish_aggregate(unsigned long long *look, unsigned long long c,
+                                                  unsigned long long agg) {
+  st_relaxed(&look[c], (c == 0 ? kFlagInc : kFlagAgg) | agg);
+}
+
+// Warp-collective.  Returns false when a bounded wait gave up or another CTA
+// aborted (the kernel then stops taking chunks and reports GPZ_ETIMEOUT).
+__device__ bool resolve_prefix(unsigned long long *look, unsigned long long c, unsigned long long agg,
+                               Control *ctl, unsigned long long &excl_out) {
   const int lane = threadIdx.x & 31;
   if (c == 0) {
-    if (lane == 0) st_relaxed(&look[0], kFlagInc | agg);
     excl_out = 0;
     return true;
   }
-  if (lane == 0) st_relaxed(&look[c], kFlagAgg | agg);
   unsigned long long excl = 0;
   long long top = (long long)c - 1;
   uint32_t spins = 0, backoff = 32;
@@ -294,7 +307,7 @@ __device__ bool lookback(unsigned long long *look, unsigned long long c, unsigne
         return false;
       }
       __nanosleep(backoff);
-      backoff = min(backoff * 2, 1024u);
+      backoff = min(backoff * 2, 256u);
       continue;
     }
     unsigned long long add = ((need >> lane) & 1u) ? (v & kValMask) : 0ull;
@@ -309,77 +322,29 @@ __device__ bool lookback(unsigned long long *look, unsigned long long c, unsigne
   return true;
 }
 
-// Stable LSD radix fallback (2-bit digits) for chunks whose ranking buckets
-// are too skewed.  Elements enter in the reference's sort input order (rank
-// r = (p%32)*32 + p/32, src/cudaWarpCompress.cu:103-118, 212-218); invalid
-// tail slots carry key 2^kb so they sort last, as UINT_MAX does there.
-template <typename T>
-__device__ void fallback_sort(CSmem<T> &s, const uint32_t (&key)[4], const uint32_t (&rel)[4],
-                              const uint32_t (&r)[4], uint32_t nvalid, uint32_t kmin, uint32_t kmax) {
-  uint32_t *keyR = reinterpret_cast<uint32_t *>(s.tmp);
-  uint32_t *relR = keyR + kChunk;
-  const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
-  const uint32_t kb = bitlen(kmax - kmin);
-  const uint32_t inv_key = 1u << kb;  // kb <= 31
-  // every slot of the chunk gets an entry: valid points by their rank, the
-  // tail ranks (points p >= nvalid) as invalid
-#pragma unroll
-  for (int e = 0; e < 4; ++e) {
-    const uint32_t p = 4 * t + e;
-    const bool v = p < nvalid;
-    keyR[r[e]] = v ? key[e] - kmin : inv_key;
-    relR[r[e]] = v ? rel[e] : 0xFFFFFFFFu;
-  }
-  __syncthreads();
-  const uint32_t nbits = kb + (nvalid < (uint32_t)kChunk ? 1u : 0u);
-  for (uint32_t bit = 0; bit < nbits; bit += 2) {
-    uint32_t kk[4], rr[4], d[4], lo[4];
-    uint32_t c4 = 0;  // four 8-bit local counters
-#pragma unroll
-    for (int e = 0; e < 4; ++e) {
-      kk[e] = keyR[4 * t + e];
-      rr[e] = relR[4 * t + e];
-      d[e] = (kk[e] >> bit) & 3u;
-      lo[e] = (c4 >> (8 * d[e])) & 0xFFu;
-      c4 += 1u << (8 * d[e]);
-    }
-    uint32_t p0 = (c4 & 0xFFu) | (((c4 >> 8) & 0xFFu) << 16);
-    uint32_t p1 = ((c4 >> 16) & 0xFFu) | (((c4 >> 24) & 0xFFu) << 16);
-    const uint32_t q0 = p0, q1 = p1;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      const uint32_t v0 = __shfl_up_sync(0xFFFFFFFFu, p0, o), v1 = __shfl_up_sync(0xFFFFFFFFu, p1, o);
-      if (lane >= o) { p0 += v0; p1 += v1; }
-    }
-    if (lane == 31) { s.fb[warp][0] = p0; s.fb[warp][1] = p1; }
-    __syncthreads();
-    uint32_t w0 = 0, w1 = 0, t0 = 0, t1 = 0;
-#pragma unroll
-    for (int w = 0; w < kWarps; ++w) {
-      const uint32_t a0 = s.fb[w][0], a1 = s.fb[w][1];
-      if (w < warp) { w0 += a0; w1 += a1; }
-      t0 += a0;
-      t1 += a1;
-    }
-    const uint32_t e0 = w0 + p0 - q0, e1 = w1 + p1 - q1;  // exclusive, packed
-    const uint32_t before[4] = {e0 & 0xFFFFu, e0 >> 16, e1 & 0xFFFFu, e1 >> 16};
-    const uint32_t tot0 = t0 & 0xFFFFu, tot1 = t0 >> 16, tot2 = t1 & 0xFFFFu;
-    const uint32_t start[4] = {0u, tot0, tot0 + tot1, tot0 + tot1 + tot2};
-    __syncthreads();
-#pragma unroll
-    for (int e = 0; e < 4; ++e) {
-      const uint32_t pos = start[d[e]] + before[d[e]] + lo[e];
-      keyR[pos] = kk[e];
-      relR[pos] = rr[e];
-    }
-    __syncthreads();
-  }
-#pragma unroll
-  for (int e = 0; e < 4; ++e) {
-    const uint32_t pos = 4 * t + e;
-    if (pos < nvalid) {
-      s.sortedK[pos] = keyR[pos] + kmin;
-      s.sortedRel[swz(pos)] = relR[pos];
+// Ascending in-place sort of a[0..n) by one warp: a bitonic network in the
+// variant whose compare-exchanges all put the minimum at the lower index (the
+// first step of each merge compares mirrored positions), so the array is
+// virtually padded with +inf up to a power of two and any exchange that
+// touches the padding is skipped.  Used for large ranking buckets.
+__device__ void warp_bitonic_u64(unsigned long long *a, int n) {
+  const int lane = threadIdx.x & 31;
+  int P = 2;
+  while (P < n) P <<= 1;
+  for (int k = 2; k <= P; k <<= 1) {
+    for (int j = k >> 1; j > 0; j >>= 1) {
+      for (int q = lane; q < (P >> 1); q += 32) {
+        const int i = ((q & ~(j - 1)) << 1) | (q & (j - 1));
+        const int p = (j == (k >> 1)) ? (i ^ (k - 1)) : (i + j);
+        if (p < n) {
+          const unsigned long long x = a[i], y = a[p];
+          if (y < x) {
+            a[i] = y;
+            a[p] = x;
+          }
+        }
+      }
+      __syncwarp();
     }
   }
 }
@@ -398,8 +363,8 @@ __device__ __forceinline__ void put_byte_word(uint8_t *stage8, uint32_t sec_off,
 }
 
 template <typename T>
-__device__ void pack_unit(CSmem<T> &s, int unit, uint32_t U, uint32_t dbits, uint32_t cbits, uint32_t rbits,
-                          uint32_t dbytes, uint32_t cbytes) {
+__device__ void pack_unit(CSmem<T> &s, uint32_t *stage, int unit, uint32_t U, uint32_t dbits, uint32_t cbits,
+                          uint32_t rbits, uint32_t dbytes, uint32_t cbytes) {
   const uint32_t ng = (U + 31u) >> 5;
   const uint32_t hd = dbits ? (dbits > 16 ? 2u : 1u) * ng : 0u;
   const uint32_t hc = cbits ? (cbits > 16 ? 2u : 1u) * ng : 0u;
@@ -421,7 +386,7 @@ __device__ void pack_unit(CSmem<T> &s, int unit, uint32_t U, uint32_t dbits, uin
   if (nb <= 8) { transpose_lo8(a); b0 = 0; cnt = nb; }
   else if (half == 0) { transpose_lo16(a); b0 = 0; cnt = min(nb, 16u); }
   else { transpose_hi16(a); b0 = 16; cnt = nb - 16; }
-  uint8_t *stage8 = reinterpret_cast<uint8_t *>(s.stage);
+  uint8_t *stage8 = reinterpret_cast<uint8_t *>(stage);
   const uint32_t bpp = (U + 7u) >> 3;
   const uint32_t sec_off = sec == 0 ? 0u : dbytes;
 #pragma unroll
@@ -429,14 +394,76 @@ __device__ void pack_unit(CSmem<T> &s, int unit, uint32_t U, uint32_t dbits, uin
     if ((uint32_t)k < cnt) {
       const uint32_t b = b0 + k;
       const uint32_t pi = nb - 1u - b;
-      if (sec == 2) s.stage[((dbytes + cbytes) >> 2) + pi * 32u + g] = a[k];
+      if (sec == 2) stage[((dbytes + cbytes) >> 2) + pi * 32u + g] = a[k];
       else put_byte_word(stage8, sec_off, bpp, pi, g, a[k]);
     }
   }
 }
 
+// Places the chunk staged in slot `sl` (warp 0): resolves its stream offset,
+// writes its offset-table entry (:1679), meta record and -- for chunk 0 -- the
+// header (:1674-1678; Double :1672-1680).  The staged copy-out follows after
+// the next CTA barrier.
+template <typename T>
+__device__ void place_staged(CSmem<T> &s, int sl, const CArgs<T> &a, unsigned long long G,
+                             unsigned long long pay_base, uint32_t seg, Control *ctl) {
+  using Tr = TT<T>;
+  constexpr bool is64 = sizeof(T) == 8;
+  const int lane = threadIdx.x & 31;
+  const unsigned long long c = s.pchunk[sl];
+  if (c == ~0ull) return;
+  const uint32_t payload = s.ppay[sl];
+  unsigned long long excl = 0;
+  const bool ok = resolve_prefix(a.look, c, payload, ctl, excl);
+  if (lane == 0) s.excl = ok ? excl : ~0ull;
+  if (!ok) return;
+  if (lane == 0) reinterpret_cast<unsigned long long *>(a.out + Tr::hdr)[c] = excl;
+  uint8_t *meta = a.out + Tr::hdr + 8ull * G + (unsigned long long)Tr::meta * c;
+  if (!is64) {
+    if (lane < 9) reinterpret_cast<uint32_t *>(meta)[lane] = s.pmeta[sl][lane];
+  } else {
+    if (lane < 8)
+      reinterpret_cast<unsigned long long *>(meta)[lane] =
+          (unsigned long long)s.pmeta[sl][2 * lane] | ((unsigned long long)s.pmeta[sl][2 * lane + 1] << 32);
+  }
+  if (c == 0) {
+    uint32_t *h = reinterpret_cast<uint32_t *>(a.out);
+    if (lane == 0) h[0] = a.dim;
+    if (lane == 1) h[1] = (uint32_t)a.n;
+    if (lane == 2) h[2] = (uint32_t)(a.n >> 32);
+    if (lane == 3) h[3] = Tr::bits;
+    if (!is64) {
+      if (lane == 4) h[4] = __float_as_uint((float)a.eb);
+      if (lane == 5) h[5] = seg;
+    } else {
+      if (lane == 4)
+        reinterpret_cast<unsigned long long *>(a.out)[2] = (unsigned long long)__double_as_longlong((double)a.eb);
+      if (lane == 6) h[6] = seg;
+      if (lane == 7) h[7] = 32u;
+    }
+  }
+  if (c == G - 1 && lane == 0) ctl->stream_bytes = pay_base + excl + payload;
+}
+
+// All threads: copies the staged payload of slot `sl` to its stream offset.
+template <typename T>
+__device__ void copy_out_staged(CSmem<T> &s, int sl, const CArgs<T> &a, unsigned long long pay_base) {
+  const unsigned long long c = s.pchunk[sl];
+  if (c == ~0ull) return;
+  const unsigned long long excl = s.excl;
+  const uint32_t payload = s.ppay[sl];
+  if (excl != ~0ull) {
+    if (pay_base + excl + payload > a.out_cap) {
+      if (threadIdx.x == 0) set_status(a.ctl, kENOSPACE);
+    } else {
+      uint32_t *dst = reinterpret_cast<uint32_t *>(a.out + pay_base + excl);
+      for (uint32_t w = threadIdx.x; w < payload / 4u; w += kThreads) dst[w] = s.stage[sl][w];
+    }
+  }
+}
+
 template <typename T, int DIM>
-__global__ void __launch_bounds__(kThreads) compress_kernel(const CArgs<T> a) {
+__global__ void __launch_bounds__(kThreads, kCompressMinBlocks) compress_kernel(const CArgs<T> a) {
   using Tr = TT<T>;
   using U = typename Tr::U;
   constexpr bool is64 = sizeof(T) == 8;
@@ -453,10 +480,17 @@ __global__ void __launch_bounds__(kThreads) compress_kernel(const CArgs<T> a) {
   const unsigned long long pay_base = Tr::hdr + 8ull * G + (unsigned long long)Tr::meta * G;
   const T *const X[3] = {a.x, a.y, a.z};
 
-  for (;;) {
-    if (t == 0) s.chunk = ld_volatile(&ctl->abort) ? 0xFFFFFFFFu : atomicAdd(&ctl->chunk_ctr, 1u);
-    __syncthreads();  // B0
+  if (t == 0) {
+    s.chunk = atomicAdd(&ctl->chunk_ctr, 1u);
+    s.pchunk[0] = s.pchunk[1] = ~0ull;
+  }
+  __syncthreads();
+  // Iteration k computes chunk c_k into stage[k & 1] and places chunk c_{k-1}
+  // (look-back + copy-out), so no CTA waits on its neighbours' sizes.
+  uint32_t it = 0;
+  for (;; ++it) {
     const unsigned long long c = s.chunk;
+    const int cur = (int)(it & 1u), prv = cur ^ 1;
     if (c >= G) break;
     const unsigned long long base = c * kChunk;
     const uint32_t nvalid = (uint32_t)min((unsigned long long)kChunk, n - base);
@@ -485,18 +519,16 @@ __global__ void __launch_bounds__(kThreads) compress_kernel(const CArgs<T> a) {
         }
     }
     {
+      // fminf / fmaxf ignore NaN and order -0.0 below +0.0, as the reference's
+      // warp reductions do (:122-139); one ordered-int transform per axis for REDUX
       const T lim = is64 ? (T)DBL_MAX : (T)FLT_MAX;
-      U mn_inv[3], mx[3];
-#pragma unroll
-      for (int d = 0; d < 3; ++d) { mn_inv[d] = (U)~ord_of(lim); mx[d] = ord_of((T)-lim); }
-#pragma unroll
-      for (int d = 0; d < DIM; ++d)
-#pragma unroll
-        for (int e = 0; e < 4; ++e)
-          if (4u * t + e < nvalid) fold_minmax<T>(v[d][e], mn_inv[d], mx[d]);
 #pragma unroll
       for (int d = 0; d < DIM; ++d) {
-        const U a0 = warp_max(mn_inv[d]), a1 = warp_max(mx[d]);
+        T mn = lim, mxv = -lim;
+#pragma unroll
+        for (int e = 0; e < 4; ++e)
+          if (4u * t + e < nvalid) { mn = fmin(mn, v[d][e]); mxv = fmax(mxv, v[d][e]); }
+        const U a0 = warp_max((U)~ord_of(mn)), a1 = warp_max(ord_of(mxv));
         if (lane == 0) { s.wmm[2 * d][warp] = a0; s.wmm[2 * d + 1][warp] = a1; }
       }
     }
@@ -584,13 +616,9 @@ __global__ void __launch_bounds__(kThreads) compress_kernel(const CArgs<T> a) {
       if (lane == 0) { s.wk[0][warp] = a0; s.wk[1][warp] = a1; s.wk[2][warp] = a2; }
     }
     __syncthreads();  // B3
-    kmin = 0xFFFFFFFFu; kmax = 0; rmax = 0;
-#pragma unroll
-    for (int w = 0; w < kWarps; ++w) {
-      kmin = min(kmin, s.wk[0][w]);
-      kmax = max(kmax, s.wk[1][w]);
-      rmax = max(rmax, s.wk[2][w]);
-    }
+    kmin = warp_min(lane < kWarps ? s.wk[0][lane & 7] : 0xFFFFFFFFu);
+    kmax = warp_max(lane < kWarps ? s.wk[1][lane & 7] : 0u);
+    rmax = warp_max(lane < kWarps ? s.wk[2][lane & 7] : 0u);
     const uint32_t rbits = max(bitlen(rmax), nvalid < (uint32_t)kChunk ? 1u : 0u);  // :200-201
 
     // ---- ranking: bucket the unique composite (block id, rank) ----
@@ -605,7 +633,6 @@ __global__ void __launch_bounds__(kThreads) compress_kernel(const CArgs<T> a) {
       if (4u * t + e < nvalid) slot[e] = atomicAdd(&s.hist[bk[e]], 1u);
     }
     __syncthreads();  // B4
-    uint32_t gmaxc;
     {
       const uint4 h = reinterpret_cast<const uint4 *>(s.hist)[t];
       const uint32_t s0 = h.x, s1 = s0 + h.y, s2 = s1 + h.z, s3 = s2 + h.w;
@@ -615,30 +642,32 @@ __global__ void __launch_bounds__(kThreads) compress_kernel(const CArgs<T> a) {
         const uint32_t q = __shfl_up_sync(0xFFFFFFFFu, inc, o);
         if (lane >= o) inc += q;
       }
-      const uint32_t mc = warp_max(max(max(h.x, h.y), max(h.z, h.w)));
-      if (lane == 31) { s.ws1[warp] = inc; s.ws2[warp] = mc; }
+      if (lane == 31) s.ws1[warp] = inc;
+      if (t == 0) s.nbig = 0;
       __syncthreads();  // B5
-      uint32_t pre = 0;
-      gmaxc = 0;
-#pragma unroll
-      for (int w = 0; w < kWarps; ++w) {
-        if (w < warp) pre += s.ws1[w];
-        gmaxc = max(gmaxc, s.ws2[w]);
-      }
+      const uint32_t pre = __reduce_add_sync(0xFFFFFFFFu, lane < warp ? s.ws1[lane & 7] : 0u);
       const uint32_t ex = pre + inc - s3;
       reinterpret_cast<uint4 *>(s.hist)[t] = make_uint4(ex, ex + s0, ex + s1, ex + s2);
       if (t == kThreads - 1) s.hist[kBuckets] = ex + s3;
+      const uint32_t hc[4] = {h.x, h.y, h.z, h.w};
+#pragma unroll
+      for (int q = 0; q < 4; ++q)
+        if (hc[q] > (uint32_t)kSmallBucket) s.big[atomicAdd(&s.nbig, 1u)] = (uint16_t)(4 * t + q);
     }
     __syncthreads();  // B6
-    if (gmaxc <= (uint32_t)kBucketLimit) {
 #pragma unroll
-      for (int e = 0; e < 4; ++e)
-        if (4u * t + e < nvalid) s.tmp[s.hist[bk[e]] + slot[e]] = C[e];
-      __syncthreads();  // B7
+    for (int e = 0; e < 4; ++e)
+      if (4u * t + e < nvalid) {
+        s.tmp[s.hist[bk[e]] + slot[e]] = C[e];
+        s.relR[r[e]] = rel[e];
+      }
+    __syncthreads();  // B7
+    // small buckets: rank = number of smaller composites in the bucket
 #pragma unroll
-      for (int e = 0; e < 4; ++e) {
-        if (4u * t + e < nvalid) {
-          const uint32_t st = s.hist[bk[e]], en = s.hist[bk[e] + 1];
+    for (int e = 0; e < 4; ++e) {
+      if (4u * t + e < nvalid) {
+        const uint32_t st = s.hist[bk[e]], en = s.hist[bk[e] + 1];
+        if (en - st <= (uint32_t)kSmallBucket) {
           uint32_t rank = 0;
           for (uint32_t j = st; j < en; ++j) rank += (s.tmp[j] < C[e]) ? 1u : 0u;
           const uint32_t pos = st + rank;
@@ -646,8 +675,17 @@ __global__ void __launch_bounds__(kThreads) compress_kernel(const CArgs<T> a) {
           s.sortedRel[swz(pos)] = rel[e];
         }
       }
-    } else {
-      fallback_sort<T>(s, key, rel, r, nvalid, kmin, kmax);
+    }
+    // large buckets: one warp sorts each slice in place
+    for (uint32_t bi = warp; bi < s.nbig; bi += kWarps) {
+      const uint32_t b = s.big[bi];
+      const uint32_t st = s.hist[b], n_b = s.hist[b + 1] - st;
+      warp_bitonic_u64(s.tmp + st, (int)n_b);
+      for (uint32_t i = lane; i < n_b; i += 32) {
+        const unsigned long long cv = s.tmp[st + i];
+        s.sortedK[st + i] = kmin + (uint32_t)(cv >> 10);
+        s.sortedRel[swz(st + i)] = s.relR[cv & 1023u];
+      }
     }
 #pragma unroll
     for (int e = 0; e < 4; ++e) {
@@ -684,15 +722,10 @@ __global__ void __launch_bounds__(kThreads) compress_kernel(const CArgs<T> a) {
       const uint32_t wd = warp_max(dm);
       if (lane == 31) { s.ws3[warp] = inc; s.ws4[warp] = wd; }
       __syncthreads();  // B9
-      uint32_t pre = 0;
-      Ucnt = 0;
-      dbits = 0;
-#pragma unroll
-      for (int w = 0; w < kWarps; ++w) {
-        if (w < warp) pre += s.ws3[w];
-        Ucnt += s.ws3[w];
-        dbits = max(dbits, s.ws4[w]);
-      }
+      const uint32_t w3 = lane < kWarps ? s.ws3[lane & 7] : 0u;
+      const uint32_t pre = __reduce_add_sync(0xFFFFFFFFu, lane < warp ? w3 : 0u);
+      Ucnt = __reduce_add_sync(0xFFFFFFFFu, w3);
+      dbits = warp_max(lane < kWarps ? s.ws4[lane & 7] : 0u);
       uint32_t u = pre + inc - cnt;
 #pragma unroll
       for (int e = 0; e < 4; ++e)
@@ -722,77 +755,60 @@ __global__ void __launch_bounds__(kThreads) compress_kernel(const CArgs<T> a) {
       if (lane == 0) s.ws5[warp] = cm;
     }
     __syncthreads();  // B11
-    cbits = 0;
-#pragma unroll
-    for (int w = 0; w < kWarps; ++w) cbits = max(cbits, s.ws5[w]);
+    cbits = warp_max(lane < kWarps ? s.ws5[lane & 7] : 0u);
 
     const uint32_t dbytes = section_bytes(Ucnt, dbits, Tr::pad);
     const uint32_t cbytes = section_bytes(Ucnt, cbits, Tr::pad);
     const uint32_t rbytes = rel_section_bytes(rbits, Tr::pad);
     const uint32_t payload = dbytes + cbytes + rbytes;
 
-    // ---- place the chunk (look-back) while the other warps pack planes ----
+    // ---- publish this chunk's size; place the previous chunk while the other
+    //      warps pack this one's bit planes ----
     if (warp == 0) {
-      unsigned long long excl = 0;
-      const bool ok = lookback(a.look, c, payload, ctl, excl);
-      if (lane == 0) s.excl = ok ? excl : ~0ull;
-      if (ok) {
-        // offset table entry (:1679) and meta record (:332-344)
-        if (lane == 0) reinterpret_cast<unsigned long long *>(a.out + Tr::hdr)[c] = excl;
-        uint8_t *meta = a.out + Tr::hdr + 8ull * G + (unsigned long long)Tr::meta * c;
-        if (!is64) {
-          uint32_t *m32 = reinterpret_cast<uint32_t *>(meta);
-          if (lane < 6) m32[lane] = __float_as_uint((float)s.mm[lane]);
-          if (lane == 6) m32[6] = s.sortedK[0];
-          if (lane == 7) m32[7] = dbits | (cbits << 16);
-          if (lane == 8) m32[8] = rbits | (Ucnt << 16);
-        } else {
-          unsigned long long *m64 = reinterpret_cast<unsigned long long *>(meta);
-          if (lane < 6) m64[lane] = (unsigned long long)__double_as_longlong((double)s.mm[lane]);
-          if (lane == 6) m64[6] = s.sortedK[0];
-          if (lane == 7)
-            m64[7] = (unsigned long long)dbits | ((unsigned long long)cbits << 16) |
-                     ((unsigned long long)rbits << 32) | ((unsigned long long)Ucnt << 48);
-        }
-        if (c == 0) {
-          // header (:1674-1678; Double :1672-1680)
-          uint32_t *h = reinterpret_cast<uint32_t *>(a.out);
-          if (lane == 0) h[0] = dim;
-          if (lane == 1) h[1] = (uint32_t)n;
-          if (lane == 2) h[2] = (uint32_t)(n >> 32);
-          if (lane == 3) h[3] = Tr::bits;
-          if (!is64) {
-            if (lane == 4) h[4] = __float_as_uint((float)eb);
-            if (lane == 5) h[5] = seg;
-          } else {
-            if (lane == 4) reinterpret_cast<unsigned long long *>(a.out)[2] = (unsigned long long)__double_as_longlong((double)eb);
-            if (lane == 6) h[6] = seg;
-            if (lane == 7) h[7] = 32u;
-          }
-        }
-        if (c == G - 1 && lane == 0) ctl->stream_bytes = pay_base + excl + payload;
-      }
+      if (lane == 0) publish_aggregate(a.look, c, payload);
+      place_staged<T>(s, prv, a, G, pay_base, seg, ctl);
     } else {
-      const int unit = t - 32;
-      pack_unit<T>(s, unit, Ucnt, dbits, cbits, rbits, dbytes, cbytes);
+      pack_unit<T>(s, s.stage[cur], t - 32, Ucnt, dbits, cbits, rbits, dbytes, cbytes);
       if (t == kThreads - 1) {
         // section padding is zero (the reference leaves it unwritten)
-        uint8_t *stage8 = reinterpret_cast<uint8_t *>(s.stage);
+        uint8_t *stage8 = reinterpret_cast<uint8_t *>(s.stage[cur]);
         const uint32_t bpp = (Ucnt + 7u) >> 3;
         for (uint32_t i = dbits * bpp; i < dbytes; ++i) stage8[i] = 0;
         for (uint32_t i = dbytes + cbits * bpp; i < dbytes + cbytes; ++i) stage8[i] = 0;
+        // meta record (:332-344 / Double :333-345) for placement next iteration
+        uint32_t *m = s.pmeta[cur];
+        if (!is64) {
+#pragma unroll
+          for (int k = 0; k < 6; ++k) m[k] = __float_as_uint((float)s.mm[k]);
+          m[6] = s.sortedK[0];
+          m[7] = dbits | (cbits << 16);
+          m[8] = rbits | (Ucnt << 16);
+        } else {
+#pragma unroll
+          for (int k = 0; k < 6; ++k) {
+            const unsigned long long b = (unsigned long long)__double_as_longlong((double)s.mm[k]);
+            m[2 * k] = (uint32_t)b;
+            m[2 * k + 1] = (uint32_t)(b >> 32);
+          }
+          m[12] = s.sortedK[0];
+          m[13] = 0;
+          m[14] = dbits | (cbits << 16);
+          m[15] = rbits | (Ucnt << 16);
+        }
+        s.pchunk[cur] = c;
+        s.ppay[cur] = payload;
       }
+      if (t == kThreads - 2) s.chunk = ld_volatile(&ctl->abort) ? 0xFFFFFFFFu : atomicAdd(&ctl->chunk_ctr, 1u);
     }
-    __syncthreads();  // B12
-    const unsigned long long excl = s.excl;
-    if (excl != ~0ull) {
-      if (pay_base + excl + payload > a.out_cap) {
-        if (t == 0) set_status(ctl, kENOSPACE);
-      } else {
-        uint32_t *dst = reinterpret_cast<uint32_t *>(a.out + pay_base + excl);
-        for (uint32_t w = t; w < payload / 4u; w += kThreads) dst[w] = s.stage[w];
-      }
-    }
+    __syncthreads();  // B12 (also publishes the next chunk id)
+    copy_out_staged<T>(s, prv, a, pay_base);
+  }
+  // drain: the chunk computed in the last iteration is still staged
+  if (it > 0) {
+    const int sl = (int)((it - 1u) & 1u);
+    if (warp == 0) place_staged<T>(s, sl, a, G, pay_base, seg, ctl);
+    __syncthreads();
+    copy_out_staged<T>(s, sl, a, pay_base);
   }
 }
 
@@ -827,7 +843,7 @@ struct __align__(16) DSmem {
 };
 
 template <typename T, int DIM>
-__global__ void __launch_bounds__(kThreads) decompress_kernel(const DArgs<T> a) {
+__global__ void __launch_bounds__(kThreads, kDecompressMinBlocks) decompress_kernel(const DArgs<T> a) {
   using Tr = TT<T>;
   constexpr bool is64 = sizeof(T) == 8;
   __shared__ DSmem<T> s;

@@ -134,9 +134,29 @@ def test_edge_cases_bit_exact(case):
     run_case(*case)
 
 
+@pytest.mark.parametrize("heavy", [17, 90, 300, 1023])
+def test_heavy_duplicate_block(heavy):
+    """A dominant cluster: `heavy` points of every chunk share one block while the
+    rest spread over the box, so one ranking bucket is large and is sorted by a warp."""
+    n = 8 * 1024 + 77
+    x, y, z = po.generate(0, n, 3, 0.0, 1000.0, 31 + heavy, np.float32)
+    rng = np.random.default_rng(heavy)
+    for c in range(0, n, 1024):
+        m = min(heavy, n - c)
+        sel = c + rng.choice(min(1024, n - c), m, replace=False)
+        x[sel] = 500.0 + rng.random(m).astype(np.float32) * 0.05
+        y[sel] = 250.0 + rng.random(m).astype(np.float32) * 0.05
+        z[sel] = 750.0 + rng.random(m).astype(np.float32) * 0.05
+    for seg in (4, 32):
+        s_o = po.compress(x, y, z, 3, float(np.float32(0.1)), seg)
+        s_g, r = _gpu_compress(x, y, z, 3, float(np.float32(0.1)), seg, "abs", 0.0)
+        assert s_g == s_o
+        _check_roundtrip(s_g, 3, 32)
+
+
 def test_fallback_sort_outlier_chunk():
-    """1023 distinct nearby block ids plus one far outlier: the ranking buckets
-    overflow and the chunk takes the stable radix fallback."""
+    """1023 nearby block ids plus one far outlier: the composite-key buckets
+    are very uneven and the large ones take the warp sort."""
     n = 4096
     x = np.zeros(n, np.float32); y = np.zeros(n, np.float32); z = np.zeros(n, np.float32)
     for c in range(4):
