@@ -17,7 +17,8 @@ constexpr int kChunk = 1024;        // points per chunk (ELEMS_PER_BLOCK, includ
 constexpr int kThreads = 256;       // threads per CTA
 constexpr int kWarps = kThreads / 32;
 constexpr int kEPT = kChunk / kThreads;   // points per thread (4)
-constexpr int kBuckets = 1024;      // ranking buckets per chunk
+constexpr int kBucketBits = 12;     // ranking buckets per chunk: 4096
+constexpr int kBuckets = 1 << kBucketBits;
 constexpr int kSmallBucket = 16;    // larger ranking buckets are sorted by a warp
 constexpr int kStageBytes = 9472;   // >= max payload: 31*128 + 11*128 + 31*128 + padding
 constexpr uint32_t kSpinLimit = 1u << 22;  // bounded waits in the look-back scan

@@ -246,14 +246,15 @@ struct CArgs {
 
 template <typename T>
 struct __align__(16) CSmem {
-  uint32_t hist[kBuckets + 16];          // bucket counts -> starts; later run starts
+  uint32_t hist[kBuckets / 2 + 16];      // packed 16-bit bucket counts -> starts; later run starts
   unsigned long long tmp[kChunk];        // composites; later delta words [0,1024) + count words [1024,2048)
   uint32_t sortedK[kChunk];
   uint32_t sortedRel[kChunk];            // swizzled
-  uint32_t relR[kChunk];                 // relative position by sort rank r
-  uint16_t big[kBuckets];                // buckets ranked by a warp sort
-  uint32_t nbig;
-  uint32_t stage[2][kStageBytes / 4 + 4];  // payload staging, two chunks in flight
+  uint16_t big[kChunk / kSmallBucket + 8];  // buckets ranked by a warp sort
+  uint32_t nbig, nwork;
+  // payload staging, two chunks in flight; stage[cur] doubles as ranking
+  // scratch (relative position by sort rank, work items) until it is packed
+  uint32_t stage[2][kStageBytes / 4 + 4];
   uint32_t pmeta[2][16];                 // meta record of the staged chunk
   unsigned long long pchunk[2];          // chunk id of the staged chunk (~0 = none)
   uint32_t ppay[2];                      // payload bytes of the staged chunk
@@ -549,7 +550,7 @@ __global__ void __launch_bounds__(kThreads, kCompressMinBlocks) compress_kernel(
         s.mm[5] = (T)0;
       }
     }
-    for (int i = t; i < kBuckets; i += kThreads) s.hist[i] = 0;
+    for (int i = t; i < kBuckets / 2 + 1; i += kThreads) s.hist[i] = 0;
     __syncthreads();  // B2
 
     // ---- quantize, block id, relative position (:141-205) ----
@@ -623,68 +624,110 @@ __global__ void __launch_bounds__(kThreads, kCompressMinBlocks) compress_kernel(
 
     // ---- ranking: bucket the unique composite (block id, rank) ----
     const unsigned long long cmax = ((unsigned long long)(kmax - kmin) << 10) | 1023ull;
-    const uint32_t shb = (uint32_t)max(0, (int)bitlen64(cmax) - 10);
+    const uint32_t shb = (uint32_t)max(0, (int)bitlen64(cmax) - kBucketBits);
     unsigned long long C[4];
     uint32_t bk[4], slot[4];
 #pragma unroll
     for (int e = 0; e < 4; ++e) {
+      const bool valid = 4u * t + e < nvalid;
       C[e] = ((unsigned long long)(key[e] - kmin) << 10) | r[e];
-      bk[e] = (uint32_t)(C[e] >> shb);
-      if (4u * t + e < nvalid) slot[e] = atomicAdd(&s.hist[bk[e]], 1u);
+      bk[e] = valid ? (uint32_t)(C[e] >> shb) : 0u;  // < kBuckets for every valid point
+      if (valid) {
+        const uint32_t h = 16u * (bk[e] & 1u);
+        slot[e] = (atomicAdd(&s.hist[bk[e] >> 1], 1u << h) >> h) & 0xFFFFu;
+      }
     }
     __syncthreads();  // B4
+    // exclusive scan of the bucket counts (16-bit, two per word); thread t owns
+    // buckets 16t..16t+15
     {
-      const uint4 h = reinterpret_cast<const uint4 *>(s.hist)[t];
-      const uint32_t s0 = h.x, s1 = s0 + h.y, s2 = s1 + h.z, s3 = s2 + h.w;
-      uint32_t inc = s3;
+      constexpr int BPT = kBuckets / kThreads;
+      const uint4 h0 = reinterpret_cast<const uint4 *>(s.hist)[2 * t];
+      const uint4 h1 = reinterpret_cast<const uint4 *>(s.hist)[2 * t + 1];
+      const uint32_t w[8] = {h0.x, h0.y, h0.z, h0.w, h1.x, h1.y, h1.z, h1.w};
+      uint32_t tot = 0;
+      uint32_t o[8];
+      uint32_t bigmask = 0;
 #pragma unroll
-      for (int o = 1; o < 32; o <<= 1) {
-        const uint32_t q = __shfl_up_sync(0xFFFFFFFFu, inc, o);
-        if (lane >= o) inc += q;
+      for (int q = 0; q < 8; ++q) {
+        const uint32_t c0 = w[q] & 0xFFFFu, c1 = w[q] >> 16;
+        o[q] = tot | ((tot + c0) << 16);
+        tot += c0 + c1;
+        bigmask |= (c0 > (uint32_t)kSmallBucket ? 1u : 0u) << (2 * q);
+        bigmask |= (c1 > (uint32_t)kSmallBucket ? 1u : 0u) << (2 * q + 1);
+      }
+      uint32_t inc = tot;
+#pragma unroll
+      for (int q = 1; q < 32; q <<= 1) {
+        const uint32_t v = __shfl_up_sync(0xFFFFFFFFu, inc, q);
+        if (lane >= q) inc += v;
       }
       if (lane == 31) s.ws1[warp] = inc;
-      if (t == 0) s.nbig = 0;
+      if (t == 0) { s.nbig = 0; s.nwork = 0; }
       __syncthreads();  // B5
-      const uint32_t pre = __reduce_add_sync(0xFFFFFFFFu, lane < warp ? s.ws1[lane & 7] : 0u);
-      const uint32_t ex = pre + inc - s3;
-      reinterpret_cast<uint4 *>(s.hist)[t] = make_uint4(ex, ex + s0, ex + s1, ex + s2);
-      if (t == kThreads - 1) s.hist[kBuckets] = ex + s3;
-      const uint32_t hc[4] = {h.x, h.y, h.z, h.w};
+      const uint32_t base = __reduce_add_sync(0xFFFFFFFFu, lane < warp ? s.ws1[lane & 7] : 0u) + inc - tot;
+      const uint32_t b2 = base | (base << 16);
 #pragma unroll
-      for (int q = 0; q < 4; ++q)
-        if (hc[q] > (uint32_t)kSmallBucket) s.big[atomicAdd(&s.nbig, 1u)] = (uint16_t)(4 * t + q);
+      for (int q = 0; q < 8; ++q) o[q] += b2;
+      reinterpret_cast<uint4 *>(s.hist)[2 * t] = make_uint4(o[0], o[1], o[2], o[3]);
+      reinterpret_cast<uint4 *>(s.hist)[2 * t + 1] = make_uint4(o[4], o[5], o[6], o[7]);
+      if (t == kThreads - 1) s.hist[kBuckets / 2] = base + tot;
+      while (bigmask) {
+        const int q = __ffs(bigmask) - 1;
+        bigmask &= bigmask - 1;
+        s.big[atomicAdd(&s.nbig, 1u)] = (uint16_t)(BPT * t + q);
+      }
     }
     __syncthreads();  // B6
-#pragma unroll
-    for (int e = 0; e < 4; ++e)
-      if (4u * t + e < nvalid) {
-        s.tmp[s.hist[bk[e]] + slot[e]] = C[e];
-        s.relR[r[e]] = rel[e];
-      }
-    __syncthreads();  // B7
-    // small buckets: rank = number of smaller composites in the bucket
+    const uint16_t *const bstart = reinterpret_cast<const uint16_t *>(s.hist);  // start of bucket b; b+1 = end
+    uint32_t *const relR = s.stage[cur];             // relative position by sort rank r
+    uint32_t *const work = s.stage[cur] + kChunk;    // own slot | start << 11 | len << 22
+    // scatter into bucket slices; a point alone in its bucket is placed at
+    // once, points of 2..16-point buckets become work items
 #pragma unroll
     for (int e = 0; e < 4; ++e) {
+      uint32_t item = 0;
+      bool is_work = false;
       if (4u * t + e < nvalid) {
-        const uint32_t st = s.hist[bk[e]], en = s.hist[bk[e] + 1];
-        if (en - st <= (uint32_t)kSmallBucket) {
-          uint32_t rank = 0;
-          for (uint32_t j = st; j < en; ++j) rank += (s.tmp[j] < C[e]) ? 1u : 0u;
-          const uint32_t pos = st + rank;
-          s.sortedK[pos] = key[e];
-          s.sortedRel[swz(pos)] = rel[e];
+        const uint32_t st = bstart[bk[e]], len = bstart[bk[e] + 1] - st;
+        if (len == 1) {
+          s.sortedK[st] = key[e];
+          s.sortedRel[swz(st)] = rel[e];
+        } else {
+          s.tmp[st + slot[e]] = C[e];
+          relR[r[e]] = rel[e];
+          is_work = len <= (uint32_t)kSmallBucket;
+          item = (st + slot[e]) | (st << 11) | (len << 22);
         }
       }
+      // warp-aggregated append to the work list
+      const uint32_t m = __ballot_sync(0xFFFFFFFFu, is_work);
+      uint32_t at = 0;
+      if (lane == 0 && m) at = atomicAdd(&s.nwork, (uint32_t)__popc(m));
+      at = __shfl_sync(0xFFFFFFFFu, at, 0);
+      if (is_work) work[at + __popc(m & ((1u << lane) - 1u))] = item;
+    }
+    __syncthreads();  // B7
+    // work items: rank = number of smaller composites in the bucket
+    for (uint32_t i = t; i < s.nwork; i += kThreads) {
+      const uint32_t wi = work[i];
+      const uint32_t own = wi & 0x7FFu, st = (wi >> 11) & 0x7FFu, len = wi >> 22;
+      const unsigned long long cv = s.tmp[own];
+      uint32_t rank = 0;
+      for (uint32_t j = 0; j < len; ++j) rank += (s.tmp[st + j] < cv) ? 1u : 0u;
+      const uint32_t pos = st + rank;
+      s.sortedK[pos] = kmin + (uint32_t)(cv >> 10);
+      s.sortedRel[swz(pos)] = relR[cv & 1023u];
     }
     // large buckets: one warp sorts each slice in place
     for (uint32_t bi = warp; bi < s.nbig; bi += kWarps) {
       const uint32_t b = s.big[bi];
-      const uint32_t st = s.hist[b], n_b = s.hist[b + 1] - st;
+      const uint32_t st = bstart[b], n_b = bstart[b + 1] - st;
       warp_bitonic_u64(s.tmp + st, (int)n_b);
       for (uint32_t i = lane; i < n_b; i += 32) {
         const unsigned long long cv = s.tmp[st + i];
         s.sortedK[st + i] = kmin + (uint32_t)(cv >> 10);
-        s.sortedRel[swz(st + i)] = s.relR[cv & 1023u];
+        s.sortedRel[swz(st + i)] = relR[cv & 1023u];
       }
     }
 #pragma unroll
