@@ -1,0 +1,374 @@
+"""Benchmark: compress + decompress of the 143,735,721-point float32 3D particle
+snapshot (70 % in 20,000 Gaussian clusters with Pareto(1.5) populations, 30 %
+uniform background, box [0,1000)^3, shuffled; relative error bound 1e-4,
+automatic segment size) on B200 GPUs.
+
+One step = one compress of the snapshot followed by one decompress of the
+resulting stream.  `value` is the uncompressed input bytes (N * 3 * 4 per rank,
+summed over ranks) divided by the step time (compress + decompress), in GB/s
+(1e9), with the inputs resident in HBM.  `e2e` is the same metric through the
+C ABI with pinned host buffers: every step copies the SoA input to the device,
+compresses, reads the stream back, copies it to the device again, decompresses
+and reads the reconstruction back.
+
+Multi-GPU: one process per GPU (torchrun); every rank compresses its own
+snapshot (seed + rank), so the work per GPU is fixed (weak scaling) and no
+collective touches the data path.  Time is the max over ranks.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+`--impl reference` times the CPU implementation of the same path on the box's
+host cores: the project's OpenMP restatement of the reference algorithm
+(oracle/), since the reference itself only has a GPU implementation.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+N_POINTS = 143_735_721
+REL_EB = 1e-4
+WORKLOAD = ("143,735,721 float32 3D points, 70% in 20,000 Gaussian clusters (sigma log-uniform "
+            "[0.5,10], Pareto(1.5) populations) + 30% uniform, box [0,1000)^3, shuffled; "
+            "rel error bound 1e-4, automatic segment size")
+METRIC = "compress & decompress GB/s (input bytes) on 1 B200, % of HBM roofline; batched vs plain"
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def traffic_from_profile():
+    """DRAM bytes per compress launch (config-2 sized) from the committed ncu summary."""
+    p = os.path.join(ROOT, "profiles", "compress_kernel_cfg2.md")
+    if not os.path.exists(p):
+        return None
+    for line in open(p):
+        if line.startswith("traffic_bytes_per_launch_cfg2:"):
+            try:
+                return float(line.split(":", 1)[1].strip())
+            except ValueError:
+                return None
+    return None
+
+
+def gen_clustered(n, seed, device):
+    """Synthetic stand-in for the SDRBench/HACC-style snapshot (not in this container)."""
+    import torch
+    g = torch.Generator(device=device)
+    g.manual_seed(seed)
+    K = 20000
+    cen = torch.rand(K, 3, generator=g, device=device) * 1000
+    sig = 0.5 * 20 ** torch.rand(K, generator=g, device=device)
+    w = (1 - torch.rand(K, generator=g, device=device)) ** (-1 / 1.5)
+    cdf = torch.cumsum(w.double(), 0)
+    ncl = int(0.7 * n)
+    u = torch.rand(ncl, generator=g, device=device, dtype=torch.float64) * cdf[-1]
+    idx = torch.searchsorted(cdf, u).clamp_(max=K - 1)
+    p = torch.empty(n, 3, device=device)
+    p[:ncl] = (cen[idx] + sig[idx, None] * torch.randn(ncl, 3, generator=g, device=device)).clamp_(0, 999.999)
+    p[ncl:] = torch.rand(n - ncl, 3, generator=g, device=device) * 1000
+    p = p[torch.randperm(n, generator=g, device=device)]
+    out = [p[:, d].contiguous() for d in range(3)]
+    del p, idx, u
+    return out
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(prefix="gpz_clocks_", suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.path or not os.path.exists(self.path):
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax.append(float(f[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        os.unlink(self.path)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_setup(n_gpus):
+    import torch
+    import torch.distributed as dist
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        from datetime import timedelta
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=torch.device("cuda", local))
+    else:
+        torch.cuda.set_device(0)
+    return world, rank, local
+
+
+def max_over_ranks(x, world):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world):
+    import torch
+    torch.cuda.synchronize()
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+    torch.cuda.synchronize()
+
+
+def cpu_baseline_run(x, y, z, steps=1):
+    """Times the OpenMP oracle (compress + decompress) on all host cores."""
+    import numpy as np
+    from oracle import pyoracle as po
+    cores = os.cpu_count() or 1
+    eb = po.rel_to_abs(x, y, z, REL_EB)
+    rel = float(np.float32(REL_EB))
+    seg, _ = po.seg_size(x, y, z, 3, 0, True, rel, eb)
+    ts = []
+    for _ in range(steps):
+        t0 = time.perf_counter()
+        s = po.compress(x, y, z, 3, eb, seg, nthreads=cores)
+        po.decompress(s, nthreads=cores)
+        ts.append(time.perf_counter() - t0)
+    return ts, cores, len(s)
+
+
+def run_reference(args):
+    """CPU implementation of the path on the host cores (rank 0 only)."""
+    import numpy as np
+    import torch
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    dev = "cuda" if torch.cuda.is_available() else "cpu"
+    x, y, z = (t.cpu().numpy() for t in gen_clustered(N_POINTS, 1234, dev))
+    if args.warmup > 0:
+        cpu_baseline_run(x, y, z, args.warmup)
+    ts, cores, sbytes = cpu_baseline_run(x, y, z, args.steps)
+    step = sum(ts) / len(ts)
+    val = N_POINTS * 12 / step / 1e9
+    line = {
+        "impl": "reference", "metric": METRIC, "value": round(val, 4), "unit": "GB/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(step * 1e3, 3), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "points": N_POINTS, "dim": 3, "error_mode": "rel", "error_bound": REL_EB},
+        "cpu_baseline": {"value": round(val, 4), "unit": "GB/s", "cores": cores, "kind": "port",
+                         "sample": f"the full snapshot ({N_POINTS} points) per step, compress + decompress, "
+                                   "OpenMP C++ restatement of the reference algorithm (the reference has no "
+                                   "CPU implementation)"},
+        "e2e": {"value": round(val, 4), "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args):
+    import numpy as np
+    import torch
+    import gpz_b200 as gz
+
+    world, rank, local = dist_setup(args.gpus)
+    dev = torch.device("cuda", local if world > 1 else 0)
+    n = N_POINTS
+    x, y, z = gen_clustered(n, 1234 + rank, dev)
+    inb = n * 3 * 4
+    eb, _ = gz.rel_to_abs(x, y, z, REL_EB)  # host-side rel->abs of the CLI, untimed as in the reference
+    rel = float(np.float32(REL_EB))
+    p = gz.make_params(n, 3, 32, eb, 0, True, rel)
+    cap = gz.stream_bound(n, 3, 32)
+    out = torch.empty(cap, dtype=torch.uint8, device=dev)
+    scr_c = torch.empty(gz.compress_scratch_bytes(n), dtype=torch.uint8, device=dev)
+    scr_d = torch.empty(256, dtype=torch.uint8, device=dev)
+    ox, oy, oz = (torch.empty(n, dtype=torch.float32, device=dev) for _ in range(3))
+    stream = torch.cuda.current_stream(dev)
+
+    # correctness gate before timing: round trip within the bound on a sample
+    r = gz.compress_into(p, x, y, z, out, scr_c)
+    rr = gz.decompress_into(out, r.stream_bytes, 32, 3, ox, oy, oz, scr_d)
+    assert r.status == 0 and rr.status == 0
+    sbytes = int(r.stream_bytes)
+    err = max(float((torch.sort(a)[0] - torch.sort(b)[0]).abs().max()) for a, b in ((x, ox), (y, oy), (z, oz)))
+    assert err <= 1.01 * eb, (err, eb)
+
+    def step(evs=None):
+        if evs is not None:
+            evs[0].record(stream)
+        gz.compress_into(p, x, y, z, out, scr_c, sync=False)
+        if evs is not None:
+            evs[1].record(stream)
+        gz.decompress_into(out, cap, 32, 3, ox, oy, oz, scr_d, sync=False)
+        if evs is not None:
+            evs[2].record(stream)
+
+    for _ in range(max(args.warmup, 3)):
+        step()
+    barrier(world)
+    evs = [[torch.cuda.Event(enable_timing=True) for _ in range(3)] for _ in range(args.steps)]
+    t0 = torch.cuda.Event(enable_timing=True)
+    t1 = torch.cuda.Event(enable_timing=True)
+    with ClockSampler(torch.cuda.current_device()) as clk:
+        barrier(world)
+        t0.record(stream)
+        for k in range(args.steps):
+            step(evs[k])
+        t1.record(stream)
+        torch.cuda.synchronize()
+    barrier(world)
+    total_ms = max_over_ranks(t0.elapsed_time(t1), world)
+    c_ms = [e[0].elapsed_time(e[1]) for e in evs]
+    d_ms = [e[1].elapsed_time(e[2]) for e in evs]
+    ms_step = total_ms / args.steps
+    value = world * inb / (ms_step * 1e-3) / 1e9
+    comp_gbs = inb / (statistics.mean(c_ms) * 1e-3) / 1e9
+    dec_gbs = inb / (statistics.mean(d_ms) * 1e-3) / 1e9
+    clocks = clk.summary()
+
+    # roofline of the dominant kernel (compress): algorithmic bytes per launch
+    # (input + stream) over its mean CUDA-event duration in the timed region
+    peak, peak_kind = peaks()
+    alg_c = inb + sbytes
+    achieved = alg_c / (statistics.mean(c_ms) * 1e-3) / 1e9
+    traffic = traffic_from_profile()
+
+    # ---- end to end through the C ABI with pinned host buffers ----
+    hx, hy, hz = (t.cpu().pin_memory() for t in (x, y, z))
+    hs = torch.empty(cap, dtype=torch.uint8).pin_memory()
+    rx, ry, rz = (torch.empty(n, dtype=torch.float32).pin_memory() for _ in range(3))
+    dx, dy, dz = (torch.empty(n, dtype=torch.float32, device=dev) for _ in range(3))
+    d_in = torch.empty(cap, dtype=torch.uint8, device=dev)
+
+    def e2e_step():
+        for h, d in ((hx, dx), (hy, dy), (hz, dz)):
+            d.copy_(h, non_blocking=True)
+        rc = gz.compress_into(p, dx, dy, dz, out, scr_c)  # reads back the result (size, status)
+        nb = int(rc.stream_bytes)
+        hs[:nb].copy_(out[:nb], non_blocking=True)
+        d_in[:nb].copy_(hs[:nb], non_blocking=True)
+        gz.decompress_into(d_in, nb, 32, 3, ox, oy, oz, scr_d, sync=False)
+        for d, h in ((ox, rx), (oy, ry), (oz, rz)):
+            h.copy_(d, non_blocking=True)
+        torch.cuda.synchronize()
+        return nb
+
+    e2e_steps = max(1, min(args.steps, 3))
+    e2e_step()
+    barrier(world)
+    te0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        nb = e2e_step()
+    te1 = time.perf_counter()
+    e2e_ms = max_over_ranks((te1 - te0) * 1e3 / e2e_steps, world)
+    e2e_val = world * inb / (e2e_ms * 1e-3) / 1e9
+
+    cpu = None
+    if world == 1 and rank == 0 and not args.no_cpu_baseline:
+        ts, cores, _ = cpu_baseline_run(hx.numpy(), hy.numpy(), hz.numpy(), 1)
+        cpu = {"value": round(inb / ts[0] / 1e9, 4), "unit": "GB/s", "cores": cores, "kind": "port",
+               "sample": f"one compress + decompress of the same {n}-point snapshot on {cores} host threads "
+                         "(OpenMP C++ restatement of the reference algorithm)"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": round(value, 3), "unit": "GB/s", "n_gpus": world, "steps": args.steps,
+            "warmup": max(args.warmup, 3), "ms_per_step": round(ms_step, 4), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded clustered generator standing in for SDRBench HACC-style snapshots)",
+            "config": {"workload": WORKLOAD, "points_per_gpu": n, "dim": 3, "error_mode": "rel",
+                       "error_bound": REL_EB, "segment_size": int(r.seg_size), "stream_bytes": sbytes,
+                       "compression_ratio": round(inb / sbytes, 4), "parallelism": f"{world} independent snapshots",
+                       "l2": "inputs (1.72 GB per GPU) larger than the 126 MB L2; no flush"},
+            "compress_gbs": round(comp_gbs, 3), "decompress_gbs": round(dec_gbs, 3),
+            "compress_ms": round(statistics.mean(c_ms), 4), "decompress_ms": round(statistics.mean(d_ms), 4),
+            "roofline": {"bound": "hbm", "kernel": "compress_kernel<float,3>", "achieved": round(achieved, 2),
+                         "peak": peak, "peak_kind": peak_kind, "unit": "GB/s", "frac": round(achieved / peak, 4),
+                         "traffic": traffic,
+                         "alg_bytes_per_launch": alg_c},
+            "gpu_launches": 3 * args.steps,
+            "clocks": clocks,
+            "e2e": {"value": round(e2e_val, 4), "unit": "GB/s", "h2d_bytes_per_step": inb + nb,
+                    "d2h_bytes_per_step": nb + inb, "steps": e2e_steps},
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

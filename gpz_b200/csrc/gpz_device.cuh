@@ -45,7 +45,7 @@ struct Control {
   uint32_t chunk_ctr;               // 24  persistent-grid work counter
   uint32_t abort;                   // 28  set when a bounded wait gives up
   uint32_t sample_done;             // 32  last-block detection for the sampling kernel
-  uint32_t pad0;                    // 36
+  uint32_t exit_ctr;                // 36  CTAs that left the persistent loop
   unsigned long long mm[6];         // 40  ordered min/max accumulators (min stored inverted)
   double out_eb;                    // 88  rel->abs result
   double out_mm[6];                 // 96  rel->abs min/max
@@ -62,6 +62,19 @@ template <> struct TT<double> {
   using U = unsigned long long;
   static constexpr uint32_t hdr = 32, meta = 64, pad = 7, bits = 64, u16_at = 56;
 };
+
+// The last CTA of a persistent grid to leave rewinds the work counter, so a
+// replay of the same launch (a profiler pass, a graph relaunch) starts over.
+__device__ __forceinline__ void rewind_work_counter(Control *ctl) {
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    if (atomicAdd(&ctl->exit_ctr, 1u) == gridDim.x - 1) {
+      atomicExch(&ctl->chunk_ctr, 0u);
+      atomicExch(&ctl->exit_ctr, 0u);
+    }
+  }
+}
 
 __device__ __forceinline__ void set_status(Control *ctl, int code) {
   atomicCAS(reinterpret_cast<int *>(&ctl->status), 0, code);

@@ -853,6 +853,7 @@ __global__ void __launch_bounds__(kThreads, kCompressMinBlocks) compress_kernel(
     __syncthreads();
     copy_out_staged<T>(s, sl, a, pay_base);
   }
+  rewind_work_counter(ctl);
 }
 
 // ===========================================================================
@@ -1163,6 +1164,7 @@ __global__ void __launch_bounds__(kThreads, kDecompressMinBlocks) decompress_ker
           if (4u * t + e < nvalid) Y[d][base + 4 * t + e] = out[d][e];
     }
   }
+  rewind_work_counter(ctl);
 }
 
 }  // namespace gpzb
