@@ -23,9 +23,9 @@ from dataclasses import dataclass
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libgpz_b200.so")
 
-GPZ_OK, GPZ_EINVAL, GPZ_ESEG, GPZ_ESTREAM, GPZ_ENOSPACE, GPZ_ECUDA, GPZ_ETIMEOUT, GPZ_ENOTSUP = range(8)
+GPZ_OK, GPZ_EINVAL, GPZ_ESEG, GPZ_ESTREAM, GPZ_ENOSPACE, GPZ_ECUDA, GPZ_ETIMEOUT, GPZ_ENOTSUP, GPZ_ELIMIT = range(9)
 GPZ_FLAG_SAFE31 = 1
-ERRORS = {1: "EINVAL", 2: "ESEG", 3: "ESTREAM", 4: "ENOSPACE", 5: "ECUDA", 6: "ETIMEOUT", 7: "ENOTSUP"}
+ERRORS = {1: "EINVAL", 2: "ESEG", 3: "ESTREAM", 4: "ENOSPACE", 5: "ECUDA", 6: "ETIMEOUT", 7: "ENOTSUP", 8: "ELIMIT"}
 
 
 class GpzError(RuntimeError):
@@ -67,6 +67,9 @@ SIGNATURES = {
     "gpz_rel_to_abs": (ctypes.c_int, [_U32, _U32, _U64, _VP, _VP, _VP, ctypes.c_double, _VP, _U64,
                                       ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double), _VP]),
     "gpz_version": (ctypes.c_char_p, []),
+    "gpz_compress_noalloc_max_points": (_U64, []),
+    "gpz_compress_noalloc": (ctypes.c_int, [ctypes.POINTER(Params), _VP, _VP, _VP, _VP, _U64,
+                                            ctypes.POINTER(Result), _VP]),
 }
 
 _lib = None

@@ -10,6 +10,7 @@
 #include <algorithm>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 
 #include "gpz_b200.h"
 #include "gpz_kernels.cuh"
@@ -254,6 +255,68 @@ int gpz_rel_to_abs(uint32_t float_bits, uint32_t dim, uint64_t n, const void *d_
   if (h_minmax6)
     for (int k = 0; k < 6; ++k) h_minmax6[k] = h.out_mm[k];
   return GPZ_OK;
+}
+
+}  // extern "C"
+
+// ===========================================================================
+// Allocation-free compress.
+//
+// Some callers cannot allocate device memory themselves: a codec plugin hosted
+// by an application that owns the whole device-memory budget and only hands
+// out the input and output buffers, or a latency-critical path where the
+// implicit device synchronisation of cudaMalloc is not acceptable.  For them
+// gpz_compress_noalloc takes its scratch (control block + one look-back word
+// per 1024-point chunk) from a fixed array compiled into this library instead
+// of from the caller.
+// ===========================================================================
+namespace {
+
+constexpr uint64_t kNoAllocScratchBytes = 4ull << 20;  // 4 MiB per GPU, held from load to exit
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+
+constexpr int kNoAllocMaxDevices = 64;
+void *g_noalloc_ptr[kNoAllocMaxDevices];
+std::mutex g_noalloc_mu;
+
+// Device address of g_noalloc_scratch on the current device.  In host code
+// the array's name only stands for a host-side shadow, so it is never handed
+// to a kernel; the address comes from cudaGetSymbolAddress, once per device,
+// with that device current.
+int noalloc_scratch(void **out) {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return GPZ_ECUDA;
+  if (dev < 0 || dev >= kNoAllocMaxDevices) return GPZ_ECUDA;
+  std::lock_guard<std::mutex> lock(g_noalloc_mu);
+  if (g_noalloc_ptr[dev] == nullptr) {
+    void *p = nullptr;
+    if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || p == nullptr) return GPZ_ECUDA;
+    g_noalloc_ptr[dev] = p;
+  }
+  *out = g_noalloc_ptr[dev];
+  return GPZ_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+uint64_t gpz_compress_noalloc_max_points(void) {
+  return ((kNoAllocScratchBytes - (uint64_t)kCtlBytes) / 8ull) * (uint64_t)kChunk;
+}
+
+int gpz_compress_noalloc(const gpz_params *params, const void *d_x, const void *d_y, const void *d_z, void *d_out,
+                         uint64_t out_capacity, gpz_result *result, void *stream) {
+  if (!params) return GPZ_EINVAL;
+  if (params->n > gpz_compress_noalloc_max_points()) return GPZ_ELIMIT;
+  void *scratch = nullptr;
+  int rc = noalloc_scratch(&scratch);
+  if (rc) return rc;
+  // gpz_compress_async clears the control block and the look-back words it
+  // uses, so the previous call's leftovers in the shared array do not matter.
+  rc = gpz_compress_async(params, d_x, d_y, d_z, d_out, out_capacity, scratch, kNoAllocScratchBytes, stream);
+  if (rc) return rc;
+  return gpz_result_get(scratch, result, stream);
 }
 
 }  // extern "C"

@@ -36,6 +36,7 @@ extern "C" {
 #define GPZ_ECUDA 5       /* a CUDA runtime call failed */
 #define GPZ_ETIMEOUT 6    /* a bounded device-side wait gave up (kernel returned early) */
 #define GPZ_ENOTSUP 7     /* feature not compiled in (e.g. nvcomp back-ends) */
+#define GPZ_ELIMIT 8      /* input larger than the fixed scratch of gpz_compress_noalloc */
 
 /* ---- parameters ------------------------------------------------------------
  * Mirrors CudaConfig (reference include/cudaCompress.cuh:16-40). */
@@ -148,6 +149,30 @@ int gpz_parse_header(const void *h_stream, uint64_t bytes, uint32_t *dim, uint64
 int gpz_rel_to_abs(uint32_t float_bits, uint32_t dim, uint64_t n, const void *d_x,
                    const void *d_y, const void *d_z, double rel, void *d_scratch,
                    uint64_t scratch_bytes, double *h_eb, double *h_minmax6, void *stream);
+
+/* ---- allocation-free compress -------------------------------------------------
+ * No counterpart in the reference (whose compress allocates with cudaMalloc on
+ * every call, src/cudaWarpCompress.cu:1631-1663).
+ *
+ * For callers that cannot allocate device memory themselves -- a codec plugin
+ * inside an application that owns the device-memory budget and only lends it
+ * the input and output buffers, or a latency-critical path that cannot take
+ * cudaMalloc's implicit device synchronisation.  Same as gpz_compress, but
+ * the scratch is a 4 MiB array compiled into the library (one copy per GPU
+ * that loads it, kept until the process exits), so the caller passes only
+ * inputs, output and stream, and nothing is allocated.
+ *
+ * Limit: n <= gpz_compress_noalloc_max_points() (536,838,144 points);
+ * larger inputs return GPZ_ELIMIT before anything is launched.
+ * The first call on each device looks up the array's device address
+ * (cudaGetSymbolAddress); make that first call before any stream capture.
+ * All calls share the one array: calls that overlap on the GPU (different
+ * streams, or different host threads on the same device) race and must be
+ * serialised by the caller.  Synchronises `stream` to return the result. */
+uint64_t gpz_compress_noalloc_max_points(void);
+int gpz_compress_noalloc(const gpz_params *params, const void *d_x, const void *d_y,
+                         const void *d_z, void *d_out, uint64_t out_capacity,
+                         gpz_result *result, void *stream);
 
 /* Library version string. */
 const char *gpz_version(void);
