@@ -222,6 +222,39 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+def run_e2e(args, world, p, hx, hy, hz, n, cap, out, scr_c, scr_d, ox, oy, oz, dev, inb):
+    """Compress + decompress through the C ABI from / to pinned host buffers, every copy timed."""
+    import torch
+    import gpz_b200 as gz
+    hs = torch.empty(cap, dtype=torch.uint8).pin_memory()
+    rx, ry, rz = (torch.empty(n, dtype=torch.float32).pin_memory() for _ in range(3))
+    dx, dy, dz = (torch.empty(n, dtype=torch.float32, device=dev) for _ in range(3))
+    d_in = torch.empty(cap, dtype=torch.uint8, device=dev)
+
+    def e2e_step():
+        for h, d in ((hx, dx), (hy, dy), (hz, dz)):
+            d.copy_(h, non_blocking=True)
+        rc = gz.compress_into(p, dx, dy, dz, out, scr_c)  # reads back the result (size, status)
+        nb = int(rc.stream_bytes)
+        hs[:nb].copy_(out[:nb], non_blocking=True)
+        d_in[:nb].copy_(hs[:nb], non_blocking=True)
+        gz.decompress_into(d_in, nb, 32, 3, ox, oy, oz, scr_d, sync=False)
+        for d, h in ((ox, rx), (oy, ry), (oz, rz)):
+            h.copy_(d, non_blocking=True)
+        torch.cuda.synchronize()
+        return nb
+
+    e2e_steps = max(1, min(args.steps, 3))
+    e2e_step()
+    barrier(world)
+    te0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        nb = e2e_step()
+    te1 = time.perf_counter()
+    e2e_ms = max_over_ranks((te1 - te0) * 1e3 / e2e_steps, world)
+    return world * inb / (e2e_ms * 1e-3) / 1e9, nb, e2e_steps
+
+
 def run_ours(args):
     import numpy as np
     import torch
@@ -229,7 +262,7 @@ def run_ours(args):
 
     world, rank, local = dist_setup(args.gpus)
     dev = torch.device("cuda", local if world > 1 else 0)
-    n = N_POINTS
+    n = args.points
     x, y, z = gen_clustered(n, 1234 + rank, dev)
     inb = n * 3 * 4
     eb, _ = gz.rel_to_abs(x, y, z, REL_EB)  # host-side rel->abs of the CLI, untimed as in the reference
@@ -292,33 +325,10 @@ def run_ours(args):
 
     # ---- end to end through the C ABI with pinned host buffers ----
     hx, hy, hz = (t.cpu().pin_memory() for t in (x, y, z))
-    hs = torch.empty(cap, dtype=torch.uint8).pin_memory()
-    rx, ry, rz = (torch.empty(n, dtype=torch.float32).pin_memory() for _ in range(3))
-    dx, dy, dz = (torch.empty(n, dtype=torch.float32, device=dev) for _ in range(3))
-    d_in = torch.empty(cap, dtype=torch.uint8, device=dev)
-
-    def e2e_step():
-        for h, d in ((hx, dx), (hy, dy), (hz, dz)):
-            d.copy_(h, non_blocking=True)
-        rc = gz.compress_into(p, dx, dy, dz, out, scr_c)  # reads back the result (size, status)
-        nb = int(rc.stream_bytes)
-        hs[:nb].copy_(out[:nb], non_blocking=True)
-        d_in[:nb].copy_(hs[:nb], non_blocking=True)
-        gz.decompress_into(d_in, nb, 32, 3, ox, oy, oz, scr_d, sync=False)
-        for d, h in ((ox, rx), (oy, ry), (oz, rz)):
-            h.copy_(d, non_blocking=True)
-        torch.cuda.synchronize()
-        return nb
-
-    e2e_steps = max(1, min(args.steps, 3))
-    e2e_step()
-    barrier(world)
-    te0 = time.perf_counter()
-    for _ in range(e2e_steps):
-        nb = e2e_step()
-    te1 = time.perf_counter()
-    e2e_ms = max_over_ranks((te1 - te0) * 1e3 / e2e_steps, world)
-    e2e_val = world * inb / (e2e_ms * 1e-3) / 1e9
+    if args.no_e2e:
+        e2e_val, nb, e2e_steps = None, sbytes, 0
+    else:
+        e2e_val, nb, e2e_steps = run_e2e(args, world, p, hx, hy, hz, n, cap, out, scr_c, scr_d, ox, oy, oz, dev, inb)
 
     cpu = None
     if world == 1 and rank == 0 and not args.no_cpu_baseline:
@@ -345,7 +355,8 @@ def run_ours(args):
                          "alg_bytes_per_launch": alg_c},
             "gpu_launches": 3 * args.steps,
             "clocks": clocks,
-            "e2e": {"value": round(e2e_val, 4), "unit": "GB/s", "h2d_bytes_per_step": inb + nb,
+            "e2e": None if e2e_val is None else
+                   {"value": round(e2e_val, 4), "unit": "GB/s", "h2d_bytes_per_step": inb + nb,
                     "d2h_bytes_per_step": nb + inb, "steps": e2e_steps},
             "cpu_baseline": cpu,
         }
@@ -363,6 +374,9 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer end-to-end timing")
+    ap.add_argument("--points", type=int, default=N_POINTS,
+                    help="points per GPU (smaller cases for profiler captures; the headline uses the default)")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)
