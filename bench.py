@@ -52,13 +52,14 @@ def peaks():
     return 6650.0, "fallback"
 
 
-def traffic_from_profile():
-    """DRAM bytes per compress launch (config-2 sized) from the committed ncu summary."""
-    p = os.path.join(ROOT, "profiles", "compress_kernel_cfg2.md")
-    if not os.path.exists(p):
+def traffic_from_profile(n):
+    """DRAM bytes per compress launch of the default 143.7M-point workload, from
+    the committed ncu summary (None for other sizes)."""
+    p = os.path.join(ROOT, "profiles", "compress_kernel_143M_f32_3d.md")
+    if n != N_POINTS or not os.path.exists(p):
         return None
     for line in open(p):
-        if line.startswith("traffic_bytes_per_launch_cfg2:"):
+        if line.startswith("traffic_bytes_per_launch:"):
             try:
                 return float(line.split(":", 1)[1].strip())
             except ValueError:
@@ -321,7 +322,7 @@ def run_ours(args):
     peak, peak_kind = peaks()
     alg_c = inb + sbytes
     achieved = alg_c / (statistics.mean(c_ms) * 1e-3) / 1e9
-    traffic = traffic_from_profile()
+    traffic = traffic_from_profile(n)
 
     # ---- end to end through the C ABI with pinned host buffers ----
     hx, hy, hz = (t.cpu().pin_memory() for t in (x, y, z))
