@@ -31,9 +31,9 @@ int num_sms() {
 }
 
 template <typename K>
-int occupancy(K kernel) {
+int occupancy(K kernel, int threads = kThreads) {
   int blocks = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, kernel, kThreads, 0) != cudaSuccess || blocks < 1)
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, kernel, threads, 0) != cudaSuccess || blocks < 1)
     blocks = 1;
   return blocks;
 }
@@ -102,20 +102,24 @@ int decompress_t(const void *d_stream, uint64_t stream_bytes, uint32_t dim, void
   a.cap = out_capacity;
   a.ctl = ctl;
   a.vec_ok = aligned16(d_x) && aligned16(d_y) && (dim == 2 || aligned16(d_z));
-  // The chunk count lives in the device header; a grid of at most one full
-  // wave loops over however many chunks there are.
-  const uint64_t bound_chunks = stream_bytes / (8ull + TT<T>::meta) + 1;
-  if (dim == 3) {
-    static int occ = 0;
-    if (!occ) occ = occupancy(decompress_kernel<T, 3>);
-    const uint64_t grid = std::min<uint64_t>((uint64_t)num_sms() * occ, bound_chunks);
-    decompress_kernel<T, 3><<<(unsigned)grid, kThreads, 0, st>>>(a);
-  } else {
-    static int occ = 0;
-    if (!occ) occ = occupancy(decompress_kernel<T, 2>);
-    const uint64_t grid = std::min<uint64_t>((uint64_t)num_sms() * occ, bound_chunks);
-    decompress_kernel<T, 2><<<(unsigned)grid, kThreads, 0, st>>>(a);
-  }
+  // The chunk count lives in the device header: one warp per chunk in a grid
+  // of at most one full wave, each warp striding over the chunks.
+  constexpr int W = DecCfg<T>::warps;
+  constexpr size_t smem = dec_smem_bytes<T>();
+  const uint64_t bound_ctas = (stream_bytes / (8ull + TT<T>::meta) + W) / W;
+  auto launch = [&](auto kernel, int &occ) -> cudaError_t {
+    if (!occ) {
+      cudaError_t e2 = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      if (e2 != cudaSuccess) return e2;
+      if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kernel, 32 * W, smem) != cudaSuccess || occ < 1) occ = 1;
+    }
+    const uint64_t grid = std::min<uint64_t>((uint64_t)num_sms() * occ, bound_ctas);
+    kernel<<<(unsigned)grid, 32 * W, smem, st>>>(a);
+    return cudaSuccess;
+  };
+  static int occ3 = 0, occ2 = 0;
+  e = dim == 3 ? launch(decompress_kernel<T, 3>, occ3) : launch(decompress_kernel<T, 2>, occ2);
+  if (e != cudaSuccess) return GPZ_ECUDA;
   return cuda_status(cudaGetLastError());
 }
 

@@ -26,11 +26,10 @@ constexpr int kCtlBytes = 256;      // control block at the head of scratch
 #ifndef GPZ_COMPRESS_MIN_BLOCKS
 #define GPZ_COMPRESS_MIN_BLOCKS 4
 #endif
-#ifndef GPZ_DECOMPRESS_MIN_BLOCKS
-#define GPZ_DECOMPRESS_MIN_BLOCKS 4
+#ifndef GPZ_DEC_MIN_CTAS_F32
+#define GPZ_DEC_MIN_CTAS_F32 4
 #endif
-constexpr int kCompressMinBlocks = GPZ_COMPRESS_MIN_BLOCKS;      // resident CTAs per SM the
-constexpr int kDecompressMinBlocks = GPZ_DECOMPRESS_MIN_BLOCKS;  // register budget is sized for
+constexpr int kCompressMinBlocks = GPZ_COMPRESS_MIN_BLOCKS;  // resident CTAs per SM the register budget is sized for
 
 // Error codes (same values as include/gpz_b200.h).
 constexpr int kOK = 0, kEINVAL = 1, kESEG = 2, kESTREAM = 3, kENOSPACE = 4, kETIMEOUT = 6;
@@ -141,9 +140,7 @@ __device__ __forceinline__ unsigned long long block_num(double range, uint32_t s
 // XORed with the group number, so the 8 threads of a load phase hit 8
 // different bank quads.
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ int swz(int i) {
-  return (i & ~31) | ((((i >> 2) & 7) ^ ((i >> 5) & 7)) << 2) | (i & 3);
-}
+__host__ __device__ __forceinline__ int swz(int i) { return i ^ ((i >> 3) & 0x1C); }
 
 // Loads the 32 values of group g (elements 32g..32g+31) from a swizzled array.
 __device__ __forceinline__ void load_group(const uint32_t *arr, int g, uint32_t (&a)[32]) {
@@ -165,115 +162,132 @@ __device__ __forceinline__ void store_group(uint32_t *arr, int g, const uint32_t
 
 // ---------------------------------------------------------------------------
 // In-register 32x32 bit transposes.  Input a[k] = value of element k; output
-// rows are bit planes: row b bit k = bit b of element k.
+// rows are bit planes: row b bit k = bit b of element k.  A transpose swaps the
+// five row-index bits with the five column-index bits one pair at a time; the
+// pair swaps commute and each is its own inverse, so the same stages (in any
+// order) also turn planes back into values.
 // The 16- and 8-bit block swaps are byte permutes (PRMT); the 4/2/1-bit
-// stages are masked XOR swaps.
+// stages are masked XOR swaps.  Host-callable so they can be checked on a CPU.
 // ---------------------------------------------------------------------------
+__host__ __device__ __forceinline__ uint32_t prmt(uint32_t a, uint32_t b, uint32_t sel) {
+#ifdef __CUDA_ARCH__
+  return __byte_perm(a, b, sel);
+#else
+  const unsigned long long x = ((unsigned long long)b << 32) | a;
+  uint32_t r = 0;
+  for (int i = 0; i < 4; ++i) r |= (uint32_t)((x >> (8 * ((sel >> (4 * i)) & 7u))) & 0xFFu) << (8 * i);
+  return r;
+#endif
+}
+
 template <int J>
-__device__ __forceinline__ void bit_stage(uint32_t &lo, uint32_t &hi) {
+__host__ __device__ __forceinline__ void bit_stage(uint32_t &lo, uint32_t &hi) {
   constexpr uint32_t m = J == 4 ? 0x0F0F0F0Fu : (J == 2 ? 0x33333333u : 0x55555555u);
   const uint32_t t = ((lo >> J) ^ hi) & m;
   lo ^= t << J;
   hi ^= t;
 }
 
-// Full transpose: a[b] = plane b for b = 0..31.
-__device__ __forceinline__ void transpose32(uint32_t (&a)[32]) {
+// The 4/2/1-bit stages over the first N words.
+template <int N>
+__host__ __device__ __forceinline__ void low_stages(uint32_t *a) {
 #pragma unroll
-  for (int k = 0; k < 16; ++k) {
-    const uint32_t lo = __byte_perm(a[k], a[k + 16], 0x5410);
-    const uint32_t hi = __byte_perm(a[k], a[k + 16], 0x7632);
-    a[k] = lo;
-    a[k + 16] = hi;
-  }
+  for (int q = 0; q < N; q += 8)
 #pragma unroll
-  for (int q = 0; q < 32; q += 16)
+    for (int k = 0; k < 4; ++k) bit_stage<4>(a[q + k], a[q + k + 4]);
+#pragma unroll
+  for (int q = 0; q < N; q += 4)
+#pragma unroll
+    for (int k = 0; k < 2; ++k) bit_stage<2>(a[q + k], a[q + k + 2]);
+#pragma unroll
+  for (int q = 0; q < N; q += 2) bit_stage<1>(a[q], a[q + 1]);
+}
+
+// Byte-swap stage between words k and k+8 of each 16-word half.
+template <int N>
+__host__ __device__ __forceinline__ void byte_stage(uint32_t *a) {
+#pragma unroll
+  for (int q = 0; q < N; q += 16)
 #pragma unroll
     for (int k = 0; k < 8; ++k) {
-      const uint32_t lo = __byte_perm(a[q + k], a[q + k + 8], 0x6240);
-      const uint32_t hi = __byte_perm(a[q + k], a[q + k + 8], 0x7351);
+      const uint32_t lo = prmt(a[q + k], a[q + k + 8], 0x6240);
+      const uint32_t hi = prmt(a[q + k], a[q + k + 8], 0x7351);
       a[q + k] = lo;
       a[q + k + 8] = hi;
     }
+}
+
+// Full transpose: a[b] = plane b for b = 0..31 (and back).
+__host__ __device__ __forceinline__ void transpose32(uint32_t (&a)[32]) {
 #pragma unroll
-  for (int q = 0; q < 32; q += 8)
-#pragma unroll
-    for (int k = 0; k < 4; ++k) bit_stage<4>(a[q + k], a[q + k + 4]);
-#pragma unroll
-  for (int q = 0; q < 32; q += 4)
-#pragma unroll
-    for (int k = 0; k < 2; ++k) bit_stage<2>(a[q + k], a[q + k + 2]);
-#pragma unroll
-  for (int q = 0; q < 32; q += 2) bit_stage<1>(a[q], a[q + 1]);
+  for (int k = 0; k < 16; ++k) {
+    const uint32_t lo = prmt(a[k], a[k + 16], 0x5410);
+    const uint32_t hi = prmt(a[k], a[k + 16], 0x7632);
+    a[k] = lo;
+    a[k + 16] = hi;
+  }
+  byte_stage<32>(a);
+  low_stages<32>(a);
 }
 
 // Planes 0..15 only (values that need <= 16 bits): a[b] = plane b, b < 16.
-__device__ __forceinline__ void transpose_lo16(uint32_t (&a)[32]) {
+__host__ __device__ __forceinline__ void transpose_lo16(uint32_t (&a)[32]) {
 #pragma unroll
-  for (int k = 0; k < 16; ++k) a[k] = __byte_perm(a[k], a[k + 16], 0x5410);
-#pragma unroll
-  for (int k = 0; k < 8; ++k) {
-    const uint32_t lo = __byte_perm(a[k], a[k + 8], 0x6240);
-    const uint32_t hi = __byte_perm(a[k], a[k + 8], 0x7351);
-    a[k] = lo;
-    a[k + 8] = hi;
-  }
-#pragma unroll
-  for (int q = 0; q < 16; q += 8)
-#pragma unroll
-    for (int k = 0; k < 4; ++k) bit_stage<4>(a[q + k], a[q + k + 4]);
-#pragma unroll
-  for (int q = 0; q < 16; q += 4)
-#pragma unroll
-    for (int k = 0; k < 2; ++k) bit_stage<2>(a[q + k], a[q + k + 2]);
-#pragma unroll
-  for (int q = 0; q < 16; q += 2) bit_stage<1>(a[q], a[q + 1]);
+  for (int k = 0; k < 16; ++k) a[k] = prmt(a[k], a[k + 16], 0x5410);
+  byte_stage<16>(a);
+  low_stages<16>(a);
 }
 
 // Planes 16..31 only: a[b - 16] = plane b.
-__device__ __forceinline__ void transpose_hi16(uint32_t (&a)[32]) {
+__host__ __device__ __forceinline__ void transpose_hi16(uint32_t (&a)[32]) {
 #pragma unroll
-  for (int k = 0; k < 16; ++k) a[k] = __byte_perm(a[k], a[k + 16], 0x7632);
-#pragma unroll
-  for (int k = 0; k < 8; ++k) {
-    const uint32_t lo = __byte_perm(a[k], a[k + 8], 0x6240);
-    const uint32_t hi = __byte_perm(a[k], a[k + 8], 0x7351);
-    a[k] = lo;
-    a[k + 8] = hi;
-  }
-#pragma unroll
-  for (int q = 0; q < 16; q += 8)
-#pragma unroll
-    for (int k = 0; k < 4; ++k) bit_stage<4>(a[q + k], a[q + k + 4]);
-#pragma unroll
-  for (int q = 0; q < 16; q += 4)
-#pragma unroll
-    for (int k = 0; k < 2; ++k) bit_stage<2>(a[q + k], a[q + k + 2]);
-#pragma unroll
-  for (int q = 0; q < 16; q += 2) bit_stage<1>(a[q], a[q + 1]);
+  for (int k = 0; k < 16; ++k) a[k] = prmt(a[k], a[k + 16], 0x7632);
+  byte_stage<16>(a);
+  low_stages<16>(a);
 }
 
 // Planes 0..7 only (values that need <= 8 bits): a[b] = plane b, b < 8.
-__device__ __forceinline__ void transpose_lo8(uint32_t (&a)[32]) {
+__host__ __device__ __forceinline__ void transpose_lo8(uint32_t (&a)[32]) {
 #pragma unroll
-  for (int k = 0; k < 16; ++k) a[k] = __byte_perm(a[k], a[k + 16], 0x5410);
+  for (int k = 0; k < 16; ++k) a[k] = prmt(a[k], a[k + 16], 0x5410);
 #pragma unroll
-  for (int k = 0; k < 8; ++k) a[k] = __byte_perm(a[k], a[k + 8], 0x6240);
-#pragma unroll
-  for (int k = 0; k < 4; ++k) bit_stage<4>(a[k], a[k + 4]);
-#pragma unroll
-  for (int q = 0; q < 8; q += 4)
-#pragma unroll
-    for (int k = 0; k < 2; ++k) bit_stage<2>(a[q + k], a[q + k + 2]);
-#pragma unroll
-  for (int q = 0; q < 8; q += 2) bit_stage<1>(a[q], a[q + 1]);
+  for (int k = 0; k < 8; ++k) a[k] = prmt(a[k], a[k + 8], 0x6240);
+  low_stages<8>(a);
+}
+
+// Inverse of transpose_lo16 for values below 2^16: planes a[b], b < 16, become
+// pairs a[k] = value k | value (k+16) << 16, k < 16.
+__host__ __device__ __forceinline__ void planes16_to_pairs(uint32_t (&a)[16]) {
+  low_stages<16>(a);
+  byte_stage<16>(a);
+}
+__host__ __device__ __forceinline__ uint32_t pair_value(const uint32_t (&a)[16], int j) {
+  return j < 16 ? (a[j] & 0xFFFFu) : (a[j - 16] >> 16);
+}
+
+// Inverse of transpose_lo8 for values below 2^8: planes a[b], b < 8, become
+// quads a[k] = value k | value (k+8) << 8 | value (k+16) << 16 | value (k+24) << 24.
+__host__ __device__ __forceinline__ void planes8_to_quads(uint32_t (&a)[8]) {
+  low_stages<8>(a);
+}
+__host__ __device__ __forceinline__ uint32_t quad_value(const uint32_t (&a)[8], int j) {
+  return (a[j & 7] >> (8 * (j >> 3))) & 0xFFu;
 }
 
 // A 32-bit plane word (bit t = element 32g+t) in the byte order of the
 // delta / count sections: element k at bit 7-(k%8) of byte k/8
 // (src/cudaWarpCompress.cu:366-378).
-__device__ __forceinline__ uint32_t to_msb_bytes(uint32_t w) { return __byte_perm(__brev(w), 0, 0x0123); }
-__device__ __forceinline__ uint32_t from_msb_bytes(uint32_t w) { return __brev(__byte_perm(w, 0, 0x0123)); }
+__host__ __device__ __forceinline__ uint32_t brev32(uint32_t w) {
+#ifdef __CUDA_ARCH__
+  return __brev(w);
+#else
+  uint32_t r = 0;
+  for (int i = 0; i < 32; ++i) r |= ((w >> i) & 1u) << (31 - i);
+  return r;
+#endif
+}
+__host__ __device__ __forceinline__ uint32_t to_msb_bytes(uint32_t w) { return prmt(brev32(w), 0, 0x0123); }
+__host__ __device__ __forceinline__ uint32_t from_msb_bytes(uint32_t w) { return brev32(prmt(w, 0, 0x0123)); }
 
 // ---------------------------------------------------------------------------
 // Exact unsigned division by a per-chunk constant (round-up magic multiplier,
@@ -311,6 +325,31 @@ struct FastDiv {
     return (t + ((n - t) >> 1)) >> s;
   }
   __host__ __device__ uint32_t mod(uint32_t n) const { return d == 0 ? n : n - div(n) * d; }
+};
+
+// Exact division of n < 2^31 by d >= 1 in three instructions:
+// q = umulhi(m, 2n) >> l, l = ceil(log2 d), m = ceil(2^(31+l) / d) < 2^32.
+// Error bound: m = 2^(31+l)/d + e with 0 <= e < 1, so m*n / 2^(31+l) exceeds
+// n/d by less than n / 2^(31+l) < 2^-l <= 1/d, which cannot carry past the
+// next integer.  d > 2^31 quotients are all 0 (m = 0).
+struct FastDiv31 {
+  uint32_t d, m, l;
+  __host__ __device__ void init(uint32_t dv) {
+    d = dv;
+    const uint32_t lg = dv <= 1 ? 0u : 32u - clz32(dv - 1u);
+    if (dv == 0 || lg >= 32) { m = 0; l = 0; return; }
+    const unsigned long long num = 1ull << (31 + lg);
+    m = (uint32_t)((num + dv - 1) / dv);
+    l = lg;
+  }
+  // n2 = 2n with n < 2^31
+  __host__ __device__ __forceinline__ uint32_t div2(uint32_t n2) const {
+#ifdef __CUDA_ARCH__
+    return __umulhi(m, n2) >> l;
+#else
+    return (uint32_t)(((unsigned long long)m * n2) >> 32) >> l;
+#endif
+  }
 };
 
 // Relaxed GPU-scope accesses for the look-back words.

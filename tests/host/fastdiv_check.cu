@@ -30,6 +30,31 @@ int main() {
     check(d, rnd());
     check(d, rnd() >> (rnd() % 32));
   }
+  // FastDiv31: n < 2^31, d >= 1
+  auto check31 = [&](uint32_t d, uint32_t n) {
+    gpzb::FastDiv31 f;
+    f.init(d);
+    ++checks;
+    if (f.div2(n + n) != n / d) {
+      if (bad < 20) printf("fd31 mismatch d=%u n=%u got %u want %u\n", d, n, f.div2(n + n), n / d);
+      ++bad;
+    }
+  };
+  for (uint32_t d : divs) {
+    if (d == 0) continue;
+    for (uint32_t n : {0u, 1u, d, d - 1u, d + 1u, 2u * d, 2u * d - 1u, 2147483647u, 2147483646u, 1073741824u})
+      if (n < 2147483648u) check31(d, n);
+    for (int i = 0; i < 20000; ++i) check31(d, rnd() >> 1);
+  }
+  for (int i = 0; i < 4000000; ++i) {
+    const uint32_t d = rnd() >> (rnd() % 32);
+    if (d == 0) continue;
+    const uint32_t n = (rnd() >> 1) >> (rnd() % 31);
+    check31(d, n);
+    const uint32_t q = n / d;  // near multiples of d
+    check31(d, q * d);
+    if (q * d) check31(d, q * d - 1u);
+  }
   printf("checks=%ld bad=%ld\n", checks, bad);
   return bad != 0;
 }
