@@ -14,6 +14,7 @@
 
 #include "gpz_b200.h"
 #include "gpz_kernels.cuh"
+#include "gpz_decode.cuh"
 
 using namespace gpzb;
 

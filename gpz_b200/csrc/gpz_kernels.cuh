@@ -6,7 +6,7 @@
 //   compress_kernel     runCompressKernel[2D] + CUB scan + header/meta assembly +
 //                       runCompactKernel (src/cudaWarpCompress.cu:32-796, 1620-1702)
 //                       fused into one persistent, single-pass kernel
-//   decompress_kernel   runDecompressKernel[2D] (src/cudaWarpCompress.cu:798-1214)
+//   (decompress_kernel: gpz_decode.cuh)
 //
 // float64 twins: src/cudaWarpCompressDouble.cu (same line ranges +/- 3).
 #pragma once
@@ -854,521 +854,6 @@ __global__ void __launch_bounds__(kThreads, kCompressMinBlocks) compress_kernel(
     copy_out_staged<T>(s, sl, a, pay_base);
   }
   rewind_work_counter(ctl);
-}
-
-// ===========================================================================
-// Decompress: one warp per chunk.
-//
-// Lane l owns unit l of every section -- elements 32l..32l+31 of the delta and
-// count planes, positions 32l..32l+31 of the relative-position planes and of
-// the output -- so the bit planes are read straight from the stream into
-// registers (one coalesced word per plane and lane) and transposed there.  The
-// only cross-lane step is the run expansion: each run writes its index at its
-// start position in a per-warp map, a max-scan over positions gives every
-// position its run, and the run's id is gathered from a per-warp id table.
-// Output rows are staged in shared memory so every store is a 512-byte
-// coalesced row segment.  Warps take chunks c = warp, warp + W, ... of a grid
-// that fits the GPU; there is no inter-warp synchronisation at all.
-// ===========================================================================
-template <typename T>
-struct DArgs {
-  const uint8_t *s;
-  unsigned long long bytes;
-  T *x, *y, *z;
-  unsigned long long cap;
-  Control *ctl;
-  int vec_ok;
-};
-
-template <typename T> struct DecCfg;
-template <> struct DecCfg<float> {
-  static constexpr int warps = 4, min_ctas = GPZ_DEC_MIN_CTAS_F32;
-  // per-warp shared words: run map -> relative positions | id table -> staged
-  // output rows | id of every position
-  static constexpr int run = 0, ids = kChunk, idhi = 0, pos = 2 * kChunk, stage = kChunk, words = 3 * kChunk;
-};
-template <> struct DecCfg<double> {
-  static constexpr int warps = 2, min_ctas = 8;
-  // run map -> relative positions | id table low / high | run of every
-  // position | staged output half-rows (16 doubles per lane)
-  static constexpr int run = 0, ids = kChunk, idhi = 2 * kChunk, pos = 3 * kChunk, stage = 4 * kChunk,
-                       words = 5 * kChunk;
-};
-template <typename T>
-constexpr size_t dec_smem_bytes() { return (size_t)DecCfg<T>::warps * DecCfg<T>::words * 4; }
-
-// Word `lane` of a delta/count byte plane that starts at byte `pos` of the
-// payload and is `bpp` bytes long: bytes 4*lane..4*lane+3, the last partial
-// word masked to the plane, returned in element order (bit t = element
-// 32*lane + t).  Only words that hold bytes of the plane are read.  The
-// aligned word under each lane (`lo`, from plane_lo) can be loaded ahead; the
-// neighbour word comes from the next lane, and lane 31 reads its own when
-// the plane reaches that far.
-__device__ __forceinline__ uint32_t plane_lo(const uint32_t *__restrict__ pw, uint32_t pos, uint32_t bpp, int lane) {
-  const uint32_t a0 = pos >> 2, last = (pos + bpp - 1u) >> 2;
-  return (a0 + (uint32_t)lane <= last) ? __ldg(pw + a0 + lane) : 0u;
-}
-__device__ __forceinline__ uint32_t plane_finish(uint32_t lo, const uint32_t *__restrict__ pw, uint32_t pos,
-                                                 uint32_t bpp, int lane) {
-  const uint32_t a0 = pos >> 2, last = (pos + bpp - 1u) >> 2, sh = (pos & 3u) << 3;
-  uint32_t hi = __shfl_down_sync(0xFFFFFFFFu, lo, 1);
-  if (lane == 31) hi = (a0 + 32u <= last) ? __ldg(pw + a0 + 32u) : 0u;
-  uint32_t w = __funnelshift_r(lo, hi, sh);
-  const int room = (int)bpp - 4 * lane;
-  if (room < 4) w = room <= 0 ? 0u : (w & (0xFFFFFFFFu >> (32 - 8 * room)));
-  return from_msb_bytes(w);
-}
-
-// Raw plane words of one section loaded ahead of use: raw[b] holds value bit
-// b's plane word (MSB plane first in the stream) when the section has at most
-// CAP planes.
-template <int CAP>
-struct PlaneWords {
-  uint32_t w[CAP];
-  bool pre;
-  // byte-plane sections (bpp != 0) and relative-position planes (bpp == 0)
-  __device__ __forceinline__ void load(const uint32_t *__restrict__ pw, uint32_t pos, uint32_t nb, uint32_t bpp,
-                                       int lane) {
-    pre = nb <= (uint32_t)CAP;
-#pragma unroll
-    for (int b = 0; b < CAP; ++b) {
-      w[b] = 0u;
-      if (pre && (uint32_t)b < nb) {
-        const uint32_t pi = nb - 1u - b;
-        w[b] = bpp ? plane_lo(pw, pos + pi * bpp, bpp, lane) : __ldg(pw + (pos >> 2) + 32u * pi + lane);
-      }
-    }
-  }
-};
-
-// Decodes this lane's 32 values of a section with nb bit planes and hands a
-// value getter val(j), j = 0..31, to `use`.  Byte-plane sections (delta,
-// count) when bpp != 0, else the relative-position section (32 little-endian
-// words per plane, word index pos/4 + 32*plane + lane).  Plane words come
-// from `raw` when it holds them, else straight from the stream.
-template <int CAP, class F>
-__device__ __forceinline__ bool decode_section(const uint32_t *__restrict__ pw, uint32_t pos, uint32_t nb,
-                                               uint32_t bpp, int lane, const PlaneWords<CAP> &raw, F &&use) {
-  auto word = [&](int b) -> uint32_t {
-    const uint32_t pi = nb - 1u - b;
-    if (b < CAP && raw.pre) {
-      const uint32_t lo = raw.w[b < CAP ? b : 0];
-      return bpp ? plane_finish(lo, pw, pos + pi * bpp, bpp, lane) : lo;
-    }
-    return bpp ? plane_finish(plane_lo(pw, pos + pi * bpp, bpp, lane), pw, pos + pi * bpp, bpp, lane)
-               : __ldg(pw + (pos >> 2) + 32u * pi + lane);
-  };
-  if (nb <= 8) {
-    uint32_t q[8];
-#pragma unroll
-    for (int b = 0; b < 8; ++b) q[b] = (uint32_t)b < nb ? word(b) : 0u;
-    planes8_to_quads(q);
-    return use([&](int j) { return quad_value(q, j); });
-  } else if (nb <= 16) {
-    uint32_t q[16];
-#pragma unroll
-    for (int b = 0; b < 16; ++b) q[b] = (uint32_t)b < nb ? word(b) : 0u;
-    planes16_to_pairs(q);
-    return use([&](int j) { return pair_value(q, j); });
-  }
-  uint32_t q[32];
-#pragma unroll
-  for (int b = 0; b < 32; ++b) q[b] = (uint32_t)b < nb ? word(b) : 0u;
-  transpose32(q);
-  return use([&](int j) { return q[j]; });
-}
-
-// Offset of the 16-byte quad m (0..7) of a lane's 32-word row: quads are XOR
-// swizzled by the row so 8 lanes touching the same quad of their rows (and
-// 8 lanes reading 8 quads of one row) hit 8 different bank groups.
-__device__ __forceinline__ uint32_t qoff(int row, int m) { return 32u * row + ((uint32_t)((m ^ row) & 7) << 2); }
-
-template <typename T>
-__device__ __forceinline__ uint32_t dec_meta_word(const uint8_t *s, unsigned long long G, unsigned long long c, int lane) {
-  using Tr = TT<T>;
-  constexpr int MW = Tr::meta / 4;
-  if (lane < MW) return reinterpret_cast<const uint32_t *>(s + Tr::hdr + 8ull * G + (unsigned long long)Tr::meta * c)[lane];
-  if (lane < MW + 2) return reinterpret_cast<const uint32_t *>(s + Tr::hdr + 8ull * c)[lane - MW];
-  return 0u;
-}
-
-// Per-chunk axis decoder: block coordinate from the run id, relative
-// position from the packed rel word, value = fma(2q+1, eb, min)
-// (src/cudaWarpCompress.cu:971-1007).  FAST uses the 3-instruction dividers,
-// valid when every id of the chunk is below 2^31.
-struct AxisDiv {
-  uint32_t bnx, bny;       // block counts (u32 arithmetic of the reference)
-  FastDiv fx, fy, fxy;     // exact dividers for any u32 id
-  FastDiv31 gx, gy, gxy;   // 3-instruction dividers for ids < 2^31
-};
-
-template <int D, bool FAST>
-__device__ __forceinline__ uint32_t block_coord(const AxisDiv &v, uint32_t id) {
-  if constexpr (FAST) {
-    const uint32_t id2 = id + id;
-    if constexpr (D == 2) return v.gxy.div2(id2);
-    const uint32_t q1 = v.gx.div2(id2);
-    if constexpr (D == 0) return id - q1 * v.bnx;
-    return q1 - v.gy.div2(q1 + q1) * v.bny;
-  } else {
-    if constexpr (D == 0) return v.fx.mod(id);
-    if constexpr (D == 1) return v.fy.mod(v.fx.div(id));
-    return v.fxy.div(id);
-  }
-}
-
-template <int D>
-__device__ __forceinline__ uint32_t rel_coord(uint32_t rp, uint32_t sh, uint32_t msk) {
-  if constexpr (D == 0) return rp & msk;
-  if constexpr (D == 1) return (rp >> sh) & msk;
-  return (2u * sh >= 32u) ? 0u : (rp >> (2u * sh));
-}
-
-// Writes this lane's staged 128-byte row segments of axis output `dst`
-// (positions p0 .. p0 + 4*EPQ - 1 for each of 8 row quads), coalesced: step k
-// writes rows 4k..4k+3, 8 lanes per row.
-template <typename T>
-__device__ __forceinline__ void copy_out_rows(const uint32_t *stage, T *dst, int lane, uint32_t half,
-                                              uint32_t nvalid, bool full) {
-  constexpr bool is64 = sizeof(T) == 8;
-  constexpr int EPQ = 16 / (int)sizeof(T);
-#pragma unroll
-  for (int k = 0; k < 8; ++k) {
-    const int row = 4 * k + (lane >> 3), qd = lane & 7;
-    const uint4 w = *reinterpret_cast<const uint4 *>(stage + qoff(row, qd));
-    const uint32_t p0 = 32u * row + 16u * half + (uint32_t)(EPQ * qd);
-    if (full) {
-      *reinterpret_cast<uint4 *>(dst + p0) = w;
-    } else {
-      const uint32_t ww[4] = {w.x, w.y, w.z, w.w};
-#pragma unroll
-      for (int e = 0; e < EPQ; ++e) {
-        if (p0 + e < nvalid) {
-          if constexpr (!is64) dst[p0 + e] = (T)__uint_as_float(ww[e]);
-          else dst[p0 + e] = (T)__hiloint2double((int)ww[2 * e + 1], (int)ww[2 * e]);
-        }
-      }
-    }
-  }
-}
-
-// float streams: ids of the 32 positions of every lane are in `pos` rows,
-// relative positions in `rel` rows; one axis at a time through `stage`.
-template <int D, bool FAST>
-__device__ __forceinline__ void reconstruct_axis_f32(const uint32_t *rel, const uint32_t *pos, uint32_t *stage,
-                                                     const AxisDiv &v, uint32_t seg, uint32_t sh, uint32_t msk,
-                                                     float eb, float mn, float *dst, int lane, uint32_t nvalid,
-                                                     bool full) {
-#pragma unroll 2
-  for (int m = 0; m < 8; ++m) {
-    const uint4 r4 = *reinterpret_cast<const uint4 *>(rel + qoff(lane, m));
-    const uint4 i4 = *reinterpret_cast<const uint4 *>(pos + qoff(lane, m));
-    const uint32_t rr[4] = {r4.x, r4.y, r4.z, r4.w}, ii[4] = {i4.x, i4.y, i4.z, i4.w};
-    uint32_t o[4];
-#pragma unroll
-    for (int e = 0; e < 4; ++e) {
-      const uint32_t q = block_coord<D, FAST>(v, ii[e]) * seg + rel_coord<D>(rr[e], sh, msk);
-      o[e] = __float_as_uint(__fmaf_rn(__uint2float_rn((q << 1) | 1u), eb, mn));
-    }
-    *reinterpret_cast<uint4 *>(stage + qoff(lane, m)) = make_uint4(o[0], o[1], o[2], o[3]);
-  }
-  __syncwarp();
-  copy_out_rows<float>(stage, dst, lane, 0u, nvalid, full);
-  __syncwarp();
-}
-
-// double streams: run of every position in `pos` rows, ids gathered from the
-// 64-bit id table per value.
-template <int D>
-__device__ __forceinline__ void reconstruct_axis_f64(const uint32_t *rel, const uint32_t *pos, const uint32_t *idlo,
-                                                     const uint32_t *idhi, uint32_t *stage, const AxisDiv &v,
-                                                     bool wide, unsigned long long bnx, unsigned long long bny,
-                                                     uint32_t seg, uint32_t sh, uint32_t msk, double eb, double mn,
-                                                     double *dst, int lane, uint32_t nvalid, bool full) {
-#pragma unroll 1
-  for (int h = 0; h < 2; ++h) {
-#pragma unroll 2
-    for (int m = 0; m < 4; ++m) {
-      const uint4 r4 = *reinterpret_cast<const uint4 *>(rel + qoff(lane, 4 * h + m));
-      const uint4 p4 = *reinterpret_cast<const uint4 *>(pos + qoff(lane, 4 * h + m));
-      const uint32_t rr[4] = {r4.x, r4.y, r4.z, r4.w}, pp[4] = {p4.x, p4.y, p4.z, p4.w};
-      unsigned long long o[4];
-#pragma unroll
-      for (int e = 0; e < 4; ++e) {
-        const int r = swz((int)pp[e]);
-        const unsigned long long id = idlo[r] | ((unsigned long long)idhi[r] << 32);
-        unsigned long long b;
-        if (!wide && (id >> 32) == 0) {
-          b = block_coord<D, false>(v, (uint32_t)id);
-        } else {
-          const unsigned long long dx = bnx, dy = bny, dxy = bnx * bny;
-          if (D == 0) b = dx ? id % dx : id;
-          else if (D == 1) { const unsigned long long q1 = dx ? id / dx : ~0ull; b = dy ? q1 % dy : q1; }
-          else b = dxy ? id / dxy : ~0ull;
-        }
-        const unsigned long long q = b * (unsigned long long)seg + rel_coord<D>(rr[e], sh, msk);
-        o[e] = (unsigned long long)__double_as_longlong(__fma_rn(__ull2double_rn((q << 1) | 1ull), eb, mn));
-      }
-      *reinterpret_cast<uint4 *>(stage + qoff(lane, 2 * m)) =
-          make_uint4((uint32_t)o[0], (uint32_t)(o[0] >> 32), (uint32_t)o[1], (uint32_t)(o[1] >> 32));
-      *reinterpret_cast<uint4 *>(stage + qoff(lane, 2 * m + 1)) =
-          make_uint4((uint32_t)o[2], (uint32_t)(o[2] >> 32), (uint32_t)o[3], (uint32_t)(o[3] >> 32));
-    }
-    __syncwarp();
-    copy_out_rows<double>(stage, dst, lane, (uint32_t)h, nvalid, full);
-    __syncwarp();
-  }
-}
-
-template <typename T, int DIM>
-__global__ void __launch_bounds__(32 * DecCfg<T>::warps, DecCfg<T>::min_ctas) decompress_kernel(const DArgs<T> a) {
-  using Tr = TT<T>;
-  using Cfg = DecCfg<T>;
-  constexpr bool is64 = sizeof(T) == 8;
-  constexpr int W = Cfg::warps;
-  constexpr uint32_t FULL = 0xFFFFFFFFu;
-  extern __shared__ __align__(16) uint32_t dec_smem[];
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  uint32_t *const sw = dec_smem + warp * Cfg::words;
-  uint32_t *const runAt = sw + Cfg::run, *const idlo = sw + Cfg::ids, *const posr = sw + Cfg::pos;
-  uint32_t *const idhi = sw + Cfg::idhi, *const stage = sw + Cfg::stage;
-  Control *ctl = a.ctl;
-  // ---- header (:1801-1828) ----
-  if (a.bytes < Tr::hdr) { if (threadIdx.x == 0) set_status(ctl, kESTREAM); return; }
-  const uint32_t dim = *reinterpret_cast<const uint32_t *>(a.s);
-  unsigned long long n;
-  memcpy(&n, a.s + 4, 8);
-  const uint32_t bits = *reinterpret_cast<const uint32_t *>(a.s + 12);
-  T eb;
-  memcpy(&eb, a.s + 16, sizeof(T));
-  const uint32_t seg = *reinterpret_cast<const uint32_t *>(a.s + 16 + sizeof(T));
-  const unsigned long long G = (n + kChunk - 1) / kChunk;
-  if (bits != Tr::bits || dim != (uint32_t)DIM || n == 0 || seg == 0 ||
-      G > (a.bytes - Tr::hdr) / (8ull + Tr::meta)) {
-    if (threadIdx.x == 0) set_status(ctl, kESTREAM);
-    return;
-  }
-  if (n > a.cap) { if (threadIdx.x == 0) set_status(ctl, kENOSPACE); return; }
-  const unsigned long long pay_base = Tr::hdr + 8ull * G + (unsigned long long)Tr::meta * G;
-  const uint32_t sh = (uint32_t)__ffs((int)seg) - 1u, msk = seg - 1u;
-  T *const Y[3] = {a.x, a.y, a.z};
-  const unsigned long long nwarps = (unsigned long long)gridDim.x * W;
-
-  unsigned long long c = (unsigned long long)blockIdx.x * W + warp;
-  uint32_t mw = c < G ? dec_meta_word<T>(a.s, G, c, lane) : 0u;
-  for (; c < G; c += nwarps) {
-    const uint32_t mwc = mw;
-    if (c + nwarps < G) mw = dec_meta_word<T>(a.s, G, c + nwarps, lane);  // next record, in flight meanwhile
-    const unsigned long long base = c * kChunk;
-    const uint32_t nvalid = (uint32_t)min((unsigned long long)kChunk, n - base);
-
-    // ---- chunk record: min/max, first id, bit widths, U, payload offset ----
-    T mm[6];
-    unsigned long long first, off;
-    uint32_t dbits, cbits, rbits, U;
-    if (!is64) {
-#pragma unroll
-      for (int k = 0; k < 6; ++k) mm[k] = (T)__uint_as_float(__shfl_sync(FULL, mwc, k));
-      first = __shfl_sync(FULL, mwc, 6);
-      const uint32_t w7 = __shfl_sync(FULL, mwc, 7), w8 = __shfl_sync(FULL, mwc, 8);
-      dbits = w7 & 0xFFFFu; cbits = w7 >> 16; rbits = w8 & 0xFFFFu; U = w8 >> 16;
-      off = __shfl_sync(FULL, mwc, 9) | ((unsigned long long)__shfl_sync(FULL, mwc, 10) << 32);
-    } else {
-#pragma unroll
-      for (int k = 0; k < 6; ++k)
-        mm[k] = (T)__hiloint2double((int)__shfl_sync(FULL, mwc, 2 * k + 1), (int)__shfl_sync(FULL, mwc, 2 * k));
-      first = __shfl_sync(FULL, mwc, 12) | ((unsigned long long)__shfl_sync(FULL, mwc, 13) << 32);
-      const uint32_t w14 = __shfl_sync(FULL, mwc, 14), w15 = __shfl_sync(FULL, mwc, 15);
-      dbits = w14 & 0xFFFFu; cbits = w14 >> 16; rbits = w15 & 0xFFFFu; U = w15 >> 16;
-      off = __shfl_sync(FULL, mwc, 16) | ((unsigned long long)__shfl_sync(FULL, mwc, 17) << 32);
-    }
-    const uint32_t db = section_bytes(U, dbits, Tr::pad), cb = section_bytes(U, cbits, Tr::pad);
-    const uint32_t rb = rel_section_bytes(rbits, Tr::pad);
-    const unsigned long long pl = (unsigned long long)db + cb + rb;
-    const bool ok = U >= 1 && U <= nvalid && dbits <= 32 && cbits <= 32 && rbits <= 32 && (off & (Tr::pad)) == 0 &&
-                    pl <= (unsigned long long)kStageBytes && pay_base <= a.bytes && off <= a.bytes - pay_base &&
-                    pl <= a.bytes - pay_base - off;
-    if (!ok) {
-      if (lane == 0) set_status(ctl, kESTREAM);
-      continue;
-    }
-    const uint32_t *pw = reinterpret_cast<const uint32_t *>(a.s + pay_base + off);
-    const uint32_t bpp = (U + 7u) >> 3;
-    // all plane words of the usual section widths in flight at once
-    PlaneWords<8> rawc;
-    PlaneWords<16> rawd, rawr;
-    rawc.load(pw, db, cbits, bpp, lane);
-    rawd.load(pw, 0u, dbits, bpp, lane);
-    rawr.load(pw, db + cb, rbits, 0u, lane);
-
-    // block counts (:831-837 / Double :835-838); lanes 0..2 build the three
-    // exact dividers at once
-    const T rx = is64 ? (T)__dsub_rn((double)mm[3], (double)mm[0]) : (T)__fsub_rn((float)mm[3], (float)mm[0]);
-    const T ry = is64 ? (T)__dsub_rn((double)mm[4], (double)mm[1]) : (T)__fsub_rn((float)mm[4], (float)mm[1]);
-    const unsigned long long bnx = block_num(rx, seg, eb, false), bny = block_num(ry, seg, eb, false);
-    AxisDiv av;
-    av.bnx = (uint32_t)bnx;
-    av.bny = (uint32_t)bny;
-    {
-      const uint32_t dv = lane == 0 ? (uint32_t)bnx : (lane == 1 ? (uint32_t)bny : (uint32_t)(bnx * bny));
-      FastDiv f;
-      f.init(dv);
-      FastDiv31 g;
-      g.init(dv);
-      av.fx.d = __shfl_sync(FULL, f.d, 0); av.fx.m = __shfl_sync(FULL, f.m, 0); av.fx.s = __shfl_sync(FULL, f.s, 0);
-      av.fy.d = __shfl_sync(FULL, f.d, 1); av.fy.m = __shfl_sync(FULL, f.m, 1); av.fy.s = __shfl_sync(FULL, f.s, 1);
-      av.fxy.d = __shfl_sync(FULL, f.d, 2); av.fxy.m = __shfl_sync(FULL, f.m, 2); av.fxy.s = __shfl_sync(FULL, f.s, 2);
-      av.gx.d = av.fx.d; av.gx.m = __shfl_sync(FULL, g.m, 0); av.gx.l = __shfl_sync(FULL, g.l, 0);
-      av.gy.d = av.fy.d; av.gy.m = __shfl_sync(FULL, g.m, 1); av.gy.l = __shfl_sync(FULL, g.l, 1);
-      av.gxy.d = av.fxy.d; av.gxy.m = __shfl_sync(FULL, g.m, 2); av.gxy.l = __shfl_sync(FULL, g.l, 2);
-    }
-    const bool wide = is64 && ((bnx >> 32) != 0 || (bny >> 32) != 0 || ((bnx * bny) >> 32) != 0);
-
-    // ---- counts -> run starts; each run writes its index at its start ----
-#pragma unroll
-    for (int m = 0; m < 8; ++m) reinterpret_cast<uint4 *>(runAt + 32 * lane)[m] = make_uint4(0u, 0u, 0u, 0u);
-    __syncwarp();
-    const bool counts_ok = decode_section(pw, db, cbits, bpp, lane, rawc, [&](auto &&val) -> bool {
-      uint32_t loc = 0;
-      bool bad = false;
-#pragma unroll
-      for (int j = 0; j < 32; ++j) {
-        const uint32_t u = 32u * lane + j, v = val(j);
-        const bool live = u < U;
-        bad |= live && (v - 1u) >= (uint32_t)kChunk;  // every run holds 1..1024 points
-        loc += live ? v : 0u;
-      }
-      uint32_t inc = loc;
-#pragma unroll
-      for (int o = 1; o < 32; o <<= 1) {
-        const uint32_t q = __shfl_up_sync(FULL, inc, o);
-        if (lane >= o) inc += q;
-      }
-      if (__any_sync(FULL, bad) || __shfl_sync(FULL, inc, 31) != nvalid) return false;
-      uint32_t st = inc - loc;
-#pragma unroll
-      for (int j = 0; j < 32; ++j) {
-        const uint32_t u = 32u * lane + j;
-        if (u < U) {
-          runAt[swz((int)st)] = u;
-          st += val(j);
-        }
-      }
-      return true;
-    });
-    if (!counts_ok) {
-      if (lane == 0) set_status(ctl, kESTREAM);
-      continue;
-    }
-
-    // ---- deltas -> id table: id[0] = first, id[u] = id[u-1] + delta[u] (:930-938) ----
-    uint32_t hi_or = 0;  // OR of the ids' bits above bit 30
-    decode_section(pw, 0u, dbits, bpp, lane, rawd, [&](auto &&val) -> bool {
-      using Acc = typename TT<T>::U;
-      Acc loc = 0;
-#pragma unroll
-      for (int j = 0; j < 32; ++j) {
-        const uint32_t u = 32u * lane + j;
-        loc += (u < U && u > 0) ? (Acc)val(j) : (Acc)0;
-      }
-      Acc inc = loc;
-#pragma unroll
-      for (int o = 1; o < 32; o <<= 1) {
-        const Acc q = __shfl_up_sync(FULL, inc, o);
-        if (lane >= o) inc += q;
-      }
-      Acc id = (Acc)first + (inc - loc);
-      uint32_t lo4[4], hi4[4];
-#pragma unroll
-      for (int j = 0; j < 32; ++j) {
-        const uint32_t u = 32u * lane + j;
-        id += (u < U && u > 0) ? (Acc)val(j) : (Acc)0;
-        lo4[j & 3] = (uint32_t)id;
-        hi4[j & 3] = (uint32_t)((unsigned long long)id >> 32);
-        if (u < U) hi_or |= (uint32_t)((unsigned long long)id >> 31);
-        if ((j & 3) == 3) {
-          *reinterpret_cast<uint4 *>(idlo + qoff(lane, j >> 2)) = make_uint4(lo4[0], lo4[1], lo4[2], lo4[3]);
-          if constexpr (is64)
-            *reinterpret_cast<uint4 *>(idhi + qoff(lane, j >> 2)) = make_uint4(hi4[0], hi4[1], hi4[2], hi4[3]);
-        }
-      }
-      return true;
-    });
-    const bool fast = !is64 && !__any_sync(FULL, hi_or != 0) && av.bnx != 0 && av.bny != 0 &&
-                      av.bnx * av.bny != 0;
-    __syncwarp();
-
-    // ---- run of every position (inclusive max-scan of the run map); float
-    // streams gather the run's id, double streams keep the run index ----
-    {
-      uint32_t run[32];
-      uint32_t mx = 0;
-#pragma unroll
-      for (int m = 0; m < 8; ++m) {
-        const uint4 v = *reinterpret_cast<const uint4 *>(runAt + qoff(lane, m));
-        mx = max(mx, v.x); run[4 * m] = mx;
-        mx = max(mx, v.y); run[4 * m + 1] = mx;
-        mx = max(mx, v.z); run[4 * m + 2] = mx;
-        mx = max(mx, v.w); run[4 * m + 3] = mx;
-      }
-      uint32_t inc = mx;
-#pragma unroll
-      for (int o = 1; o < 32; o <<= 1) {
-        const uint32_t q = __shfl_up_sync(FULL, inc, o);
-        if (lane >= o) inc = max(inc, q);
-      }
-      uint32_t pre = __shfl_up_sync(FULL, inc, 1);
-      if (lane == 0) pre = 0;
-#pragma unroll
-      for (int m = 0; m < 8; ++m) {
-        uint32_t o[4];
-#pragma unroll
-        for (int e = 0; e < 4; ++e) {
-          const uint32_t r = max(run[4 * m + e], pre);
-          o[e] = is64 ? r : idlo[swz((int)r)];
-        }
-        *reinterpret_cast<uint4 *>(posr + qoff(lane, m)) = make_uint4(o[0], o[1], o[2], o[3]);
-      }
-    }
-
-    // ---- relative positions of this lane's 32 positions -> own run-map row ----
-    decode_section(pw, db + cb, rbits, 0u, lane, rawr, [&](auto &&val) -> bool {
-#pragma unroll
-      for (int m = 0; m < 8; ++m)
-        *reinterpret_cast<uint4 *>(runAt + qoff(lane, m)) =
-            make_uint4(val(4 * m), val(4 * m + 1), val(4 * m + 2), val(4 * m + 3));
-      return true;
-    });
-    __syncwarp();  // id table reads done: its rows become output staging (float streams)
-
-    // ---- reconstruct (:971-1007) ----
-    const bool full = nvalid == (uint32_t)kChunk && a.vec_ok;
-    if constexpr (!is64) {
-      const float e = (float)eb;
-      float *const X0 = (float *)Y[0] + base, *const X1 = (float *)Y[1] + base, *const X2 = (float *)Y[2] + base;
-      if (fast) {
-        reconstruct_axis_f32<0, true>(runAt, posr, stage, av, seg, sh, msk, e, (float)mm[0], X0, lane, nvalid, full);
-        reconstruct_axis_f32<1, true>(runAt, posr, stage, av, seg, sh, msk, e, (float)mm[1], X1, lane, nvalid, full);
-        if (DIM == 3)
-          reconstruct_axis_f32<2, true>(runAt, posr, stage, av, seg, sh, msk, e, (float)mm[2], X2, lane, nvalid, full);
-      } else {
-        reconstruct_axis_f32<0, false>(runAt, posr, stage, av, seg, sh, msk, e, (float)mm[0], X0, lane, nvalid, full);
-        reconstruct_axis_f32<1, false>(runAt, posr, stage, av, seg, sh, msk, e, (float)mm[1], X1, lane, nvalid, full);
-        if (DIM == 3)
-          reconstruct_axis_f32<2, false>(runAt, posr, stage, av, seg, sh, msk, e, (float)mm[2], X2, lane, nvalid, full);
-      }
-    } else {
-      const double e = (double)eb;
-      double *const X0 = (double *)Y[0] + base, *const X1 = (double *)Y[1] + base, *const X2 = (double *)Y[2] + base;
-      reconstruct_axis_f64<0>(runAt, posr, idlo, idhi, stage, av, wide, bnx, bny, seg, sh, msk, e, (double)mm[0], X0,
-                              lane, nvalid, full);
-      reconstruct_axis_f64<1>(runAt, posr, idlo, idhi, stage, av, wide, bnx, bny, seg, sh, msk, e, (double)mm[1], X1,
-                              lane, nvalid, full);
-      if (DIM == 3)
-        reconstruct_axis_f64<2>(runAt, posr, idlo, idhi, stage, av, wide, bnx, bny, seg, sh, msk, e, (double)mm[2],
-                                X2, lane, nvalid, full);
-    }
-  }
 }
 
 }  // namespace gpzb
