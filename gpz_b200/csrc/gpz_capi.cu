@@ -14,6 +14,7 @@
 
 #include "gpz_b200.h"
 #include "gpz_kernels.cuh"
+#include "gpz_encode.cuh"
 #include "gpz_decode.cuh"
 
 using namespace gpzb;
@@ -72,17 +73,22 @@ int compress_t(const gpz_params *p, const void *d_x, const void *d_y, const void
   a.eb = eb;
   a.dim = p->dim;
   a.vec_ok = aligned16(d_x) && aligned16(d_y) && (p->dim == 2 || aligned16(d_z));
-  if (p->dim == 3) {
-    static int occ = 0;
-    if (!occ) occ = occupancy(compress_kernel<T, 3>);
-    const uint64_t grid = std::min<uint64_t>(G, (uint64_t)num_sms() * occ);
-    compress_kernel<T, 3><<<(unsigned)grid, kThreads, 0, st>>>(a);
-  } else {
-    static int occ = 0;
-    if (!occ) occ = occupancy(compress_kernel<T, 2>);
-    const uint64_t grid = std::min<uint64_t>(G, (uint64_t)num_sms() * occ);
-    compress_kernel<T, 2><<<(unsigned)grid, kThreads, 0, st>>>(a);
-  }
+  // persistent grid: one CTA per kEncWarps chunks in flight
+  constexpr size_t smem = enc_smem_bytes();
+  auto launch = [&](auto kernel, int &occ) -> cudaError_t {
+    if (!occ) {
+      cudaError_t e2 = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      if (e2 != cudaSuccess) return e2;
+      if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kernel, 32 * kEncWarps, smem) != cudaSuccess || occ < 1)
+        occ = 1;
+    }
+    const uint64_t grid = std::min<uint64_t>((G + kEncWarps - 1) / kEncWarps, (uint64_t)num_sms() * occ);
+    kernel<<<(unsigned)grid, 32 * kEncWarps, smem, st>>>(a);
+    return cudaSuccess;
+  };
+  static int occ3 = 0, occ2 = 0;
+  e = p->dim == 3 ? launch(compress_kernel<T, 3>, occ3) : launch(compress_kernel<T, 2>, occ2);
+  if (e != cudaSuccess) return GPZ_ECUDA;
   return cuda_status(cudaGetLastError());
 }
 

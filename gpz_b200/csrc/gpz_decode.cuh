@@ -51,12 +51,6 @@ template <> struct DecCfg<double> {
 template <typename T>
 constexpr size_t dec_smem_bytes() { return (size_t)DecCfg<T>::warps * DecCfg<T>::words * 4; }
 
-// Offset of the 16-byte quad m (0..7) of a lane's 32-word row: quads are XOR
-// swizzled by the row so 8 lanes touching the same quad of their rows (and
-// 8 lanes reading 8 quads of one row) hit 8 different bank groups.  swz()
-// maps an element index to the same place.
-__device__ __forceinline__ uint32_t qoff(int row, int m) { return 32u * row + ((uint32_t)((m ^ row) & 7) << 2); }
-
 // ---------------------------------------------------------------------------
 // Bit planes.  Delta and count planes are ceil(U/8) bytes each, MSB plane
 // first, element k at bit 7-(k%8) of byte k/8 (src/cudaWarpCompress.cu:366-378);

@@ -142,6 +142,11 @@ __device__ __forceinline__ unsigned long long block_num(double range, uint32_t s
 // ---------------------------------------------------------------------------
 __host__ __device__ __forceinline__ int swz(int i) { return i ^ ((i >> 3) & 0x1C); }
 
+// Offset of the 16-byte quad m (0..7) of row `row` in the same layout: 8 lanes
+// touching the same quad of their rows (or 8 quads of one row) hit 8
+// different bank groups.
+__device__ __forceinline__ uint32_t qoff(int row, int m) { return 32u * row + ((uint32_t)((m ^ row) & 7) << 2); }
+
 // Loads the 32 values of group g (elements 32g..32g+31) from a swizzled array.
 __device__ __forceinline__ void load_group(const uint32_t *arr, int g, uint32_t (&a)[32]) {
   const uint4 *p = reinterpret_cast<const uint4 *>(arr + 32 * g);

@@ -1,0 +1,591 @@
+// gpz_encode.cuh -- compress kernel of the B200 GPZ codec.
+//
+//   compress_kernel   runCompressKernel[2D] + CUB scan + header/meta assembly
+//                     + runCompactKernel (reference src/cudaWarpCompress.cu:32-796,
+//                     1620-1702; float64 twin src/cudaWarpCompressDouble.cu)
+//                     fused into one persistent, single-pass kernel.
+//
+// One warp encodes one 1024-point chunk.  Lane l holds the 32 points whose
+// stable rank r(p) = (p % 32) * 32 + p / 32 (the reference's sort order for
+// equal block ids) is 32l..32l+31, so the composite (block id, r) is unique
+// and a point's register index is its rank within the lane.  The warp:
+//   1. loads and quantizes one axis at a time (block id in registers, the
+//      relative position accumulated in a shared row per lane);
+//   2. ranks the composites: 2048 buckets on the top bits, counted with
+//      shared atomics, placed by bucket start + arrival slot, and every
+//      multi-point bucket put in order afterwards (insertion by its owning
+//      lane, or a warp bitonic network for buckets above 16 points);
+//   3. finds the runs of equal ids (unique ids, deltas, counts) and compacts
+//      them through shared memory so lane l holds runs 32l..32l+31;
+//   4. transposes deltas, counts and relative positions into bit planes in
+//      registers and assembles the payload in its shared region.
+// The 4 warps of a CTA take 4 consecutive chunks together; one decoupled
+// look-back per group places the group's payloads in the stream.
+#pragma once
+
+#include <cfloat>
+#include "gpz_kernels.cuh"
+
+namespace gpzb {
+
+constexpr int kEncWarps = 4;              // chunks (warps) per CTA
+constexpr int kEncBucketBits = 11;        // ranking buckets per chunk: 2048
+constexpr int kEncSmall = 16;             // larger buckets are sorted by the whole warp
+constexpr int kEncWords = 3 * kChunk;     // per-warp shared words (12 KB)
+static_assert(kStageBytes <= kEncWords * 4, "payload staging must fit the warp region");
+
+struct EncGroup {
+  uint32_t sz[kEncWarps];    // payload bytes of each warp's chunk
+  unsigned long long goff;   // stream offset of the group (~0: look-back gave up)
+  unsigned long long next;   // first chunk of the next group
+};
+
+constexpr size_t enc_smem_bytes() { return (size_t)kEncWarps * kEncWords * 4; }
+
+// Index of bucket-count word w, position / run u, ... in a swizzled 1024-word
+// array (rows of 32 words, 16-byte quads XORed by the row).
+__device__ __forceinline__ uint32_t sx(uint32_t i) { return (uint32_t)swz((int)i); }
+
+// Ascending in-place bitonic sort of the n = hi - lo values a[sx(lo..hi)) by
+// one warp (variant whose exchanges all put the minimum at the lower index,
+// virtually padded with +inf up to a power of two).
+__device__ void warp_bitonic_u32(uint32_t *a, uint32_t lo, uint32_t n, int lane) {
+  uint32_t P = 2;
+  while (P < n) P <<= 1;
+  for (uint32_t k = 2; k <= P; k <<= 1) {
+    for (uint32_t j = k >> 1; j > 0; j >>= 1) {
+      for (uint32_t q = lane; q < (P >> 1); q += 32) {
+        const uint32_t i = ((q & ~(j - 1)) << 1) | (q & (j - 1));
+        const uint32_t p = (j == (k >> 1)) ? (i ^ (k - 1)) : (i + j);
+        if (p < n) {
+          const uint32_t x = a[sx(lo + i)], y = a[sx(lo + p)];
+          if (y < x) {
+            a[sx(lo + i)] = y;
+            a[sx(lo + p)] = x;
+          }
+        }
+      }
+      __syncwarp();
+    }
+  }
+}
+
+// Start of bucket b (b = 2048 gives the number of ranked points).
+__device__ __forceinline__ uint32_t bucket_start(const uint32_t *hist, uint32_t b, uint32_t total) {
+  if (b >= (1u << kEncBucketBits)) return total;
+  return (hist[sx(b >> 1)] >> ((b & 1u) << 4)) & 0xFFFFu;
+}
+
+// Writes one 32-element plane word of a delta / count section into the
+// staged payload: bytes 4*lane.. of the plane, MSB-first bit order
+// (src/cudaWarpCompress.cu:357-408), only the bytes the plane has.
+__device__ __forceinline__ void put_plane_bytes(uint8_t *stage8, uint32_t pos, uint32_t bpp, uint32_t word,
+                                                int lane) {
+  const int room = (int)bpp - 4 * lane;
+  if (room <= 0) return;
+  const uint32_t w = to_msb_bytes(word);
+  uint8_t *d = stage8 + pos + 4u * lane;
+  d[0] = (uint8_t)w;
+  if (room > 1) d[1] = (uint8_t)(w >> 8);
+  if (room > 2) d[2] = (uint8_t)(w >> 16);
+  if (room > 3) d[3] = (uint8_t)(w >> 24);
+}
+
+// Bit planes of this lane's 32 values (v: value of element j) into the staged
+// payload: byte planes at pos0 + pi*bpp (bpp != 0) or 32-word planes at word
+// pos0/4 + 32*pi + lane (bpp == 0), MSB plane first.  v is clobbered.
+__device__ __forceinline__ void put_planes(uint32_t *stage, uint32_t pos0, uint32_t nb, uint32_t bpp,
+                                           uint32_t (&v)[32], int lane) {
+  uint8_t *stage8 = reinterpret_cast<uint8_t *>(stage);
+  auto put = [&](uint32_t b, uint32_t w) {
+    const uint32_t pi = nb - 1u - b;
+    if (bpp) put_plane_bytes(stage8, pos0 + pi * bpp, bpp, w, lane);
+    else stage[(pos0 >> 2) + 32u * pi + lane] = w;
+  };
+  if (nb <= 8) {
+    transpose_lo8(v);
+#pragma unroll
+    for (int b = 0; b < 8; ++b)
+      if ((uint32_t)b < nb) put(b, v[b]);
+  } else if (nb <= 16) {
+    transpose_lo16(v);
+#pragma unroll
+    for (int b = 0; b < 16; ++b)
+      if ((uint32_t)b < nb) put(b, v[b]);
+  } else {
+    transpose32(v);
+#pragma unroll
+    for (int b = 0; b < 32; ++b)
+      if ((uint32_t)b < nb) put(b, v[b]);
+  }
+}
+
+// Encodes chunk c into the warp's region `sw`; returns the payload bytes and
+// leaves the meta record in meta[] (word k of the record in lane k).
+template <typename T, int DIM>
+__device__ uint32_t encode_chunk(const CArgs<T> &a, unsigned long long c, uint32_t *sw, uint32_t seg, uint32_t sh,
+                                 uint32_t msk, T inv, uint32_t &meta_word, int lane) {
+  using Tr = TT<T>;
+  using UO = typename Tr::U;
+  constexpr bool is64 = sizeof(T) == 8;
+  constexpr uint32_t FULL = 0xFFFFFFFFu;
+  const T eb = a.eb;
+  const unsigned long long n = a.n;
+  const unsigned long long base = c * kChunk;
+  const uint32_t nvalid = (uint32_t)min((unsigned long long)kChunk, n - base);
+  const bool full = nvalid == (uint32_t)kChunk;
+  // per-warp words: [0,1024) ranked composites -> run starts -> staged payload;
+  // [1024,2048) bucket counts -> deltas -> staged payload; [2048,3072)
+  // relative positions by rank r (staged payload only past 8 KB, after use)
+  uint32_t *const S = sw, *const hist = sw + kChunk, *const relR = sw + 2 * kChunk;
+  const T *const X[3] = {a.x, a.y, a.z};
+
+  // ---- 1. quantize one axis at a time (:104-205) ----
+  uint32_t key[32];
+  T mm[6];
+  unsigned long long bnx = 0, bny = 0, bound = 0;
+  uint32_t rmax = 0;
+#pragma unroll
+  for (int d = 0; d < DIM; ++d) {
+    T v[32];
+    const T *src = X[d] + base;
+#pragma unroll
+    for (int j = 0; j < 32; ++j) {
+      const uint32_t p = 32u * j + lane;
+      v[j] = (full || p < nvalid) ? src[p] : (T)0;
+    }
+    // fmin / fmax ignore NaN and order -0.0 below +0.0, as the reference's
+    // warp reductions do (:122-139)
+    const T lim = is64 ? (T)DBL_MAX : (T)FLT_MAX;
+    T mn = lim, mx = -lim;
+#pragma unroll
+    for (int j = 0; j < 32; ++j)
+      if (full || 32u * j + lane < nvalid) { mn = fmin(mn, v[j]); mx = fmax(mx, v[j]); }
+    mn = from_ord((UO)~warp_max((UO)~ord_of(mn)));
+    mx = from_ord(warp_max(ord_of(mx)));
+    mm[d] = mn;
+    mm[3 + d] = mx;
+    const T range = is64 ? (T)__dsub_rn((double)mx, (double)mn) : (T)__fsub_rn((float)mx, (float)mn);
+    if (d == 0) bnx = block_num(range, seg, eb, is64 && DIM == 2);
+    if (d == 1) bny = block_num(range, seg, eb, false);
+    const T nmn = is64 ? (T)__dmul_rn(-(double)mn, (double)inv) : (T)__fmul_rn(-(float)mn, (float)inv);
+    // id_overflow: the chunk's largest quantized corner (u64 arithmetic)
+    const unsigned long long qm = is64 ? __double2ull_rz(__fma_rn((double)mx, (double)inv, (double)nmn))
+                                       : (unsigned long long)__float2uint_rz(__fmaf_rn((float)mx, (float)inv, (float)nmn));
+    bound += (qm >> sh) * (d == 0 ? 1ull : (d == 1 ? bnx : bnx * bny));
+    // block id (mod 2^32, masked to 31 bits at the end) and relative position
+    const uint32_t kmul = d == 0 ? 1u : (d == 1 ? (uint32_t)bnx : (uint32_t)(bnx * bny));
+    const uint32_t rmul = d == 0 ? 1u : (d == 1 ? seg : seg * seg);
+#pragma unroll
+    for (int m = 0; m < 8; ++m) {
+      uint32_t rq[4];
+#pragma unroll
+      for (int e = 0; e < 4; ++e) {
+        const int j = 4 * m + e;
+        uint32_t kq, r;
+        if constexpr (!is64) {
+          const uint32_t q = __float2uint_rz(__fmaf_rn((float)v[j], (float)inv, (float)nmn));
+          kq = q >> sh;
+          r = q & msk;
+        } else {
+          const unsigned long long q = __double2ull_rz(__fma_rn((double)v[j], (double)inv, (double)nmn));
+          kq = (uint32_t)(q >> sh);
+          r = (uint32_t)(q & msk);
+        }
+        key[j] = d == 0 ? kq : key[j] + kq * kmul;
+        rq[e] = r * rmul;
+      }
+      uint4 *row = reinterpret_cast<uint4 *>(relR + qoff(lane, m));
+      if (d > 0) {
+        const uint4 o = *row;
+        rq[0] += o.x; rq[1] += o.y; rq[2] += o.z; rq[3] += o.w;
+      }
+      if (d == DIM - 1) {
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+          rq[e] &= 0x7FFFFFFFu;
+          if (full || 32u * (4 * m + e) + lane < nvalid) rmax = max(rmax, rq[e]);
+        }
+      }
+      *row = make_uint4(rq[0], rq[1], rq[2], rq[3]);
+    }
+  }
+  if (DIM == 2) { mm[2] = (T)0; mm[5] = (T)0; }  // 2D meta carries z = 0 (:518, :521)
+  if (lane == 0 && bound > 0x7FFFFFFFull) a.ctl->id_overflow = 1u;
+  uint32_t kmin = FULL, kmax = 0;
+#pragma unroll
+  for (int j = 0; j < 32; ++j) {
+    key[j] &= 0x7FFFFFFFu;
+    if (full || 32u * j + lane < nvalid) { kmin = min(kmin, key[j]); kmax = max(kmax, key[j]); }
+  }
+  kmin = warp_min(kmin);
+  kmax = warp_max(kmax);
+  rmax = warp_max(rmax);
+  const uint32_t rbits = max(bitlen(rmax), nvalid < (uint32_t)kChunk ? 1u : 0u);  // :200-201
+
+  // ---- 2. rank the composites (block id - kmin) << 10 | r ----
+  const unsigned long long cmax = ((unsigned long long)(kmax - kmin) << 10) | 1023ull;
+  const uint32_t cbits_all = bitlen64(cmax);
+  const uint32_t shb = cbits_all > (uint32_t)kEncBucketBits ? cbits_all - kEncBucketBits : 0u;
+  const bool wide = cbits_all > 32u;  // then S keeps the composite's bits below the bucket
+#pragma unroll
+  for (int m = 0; m < 8; ++m) reinterpret_cast<uint4 *>(hist + 32 * lane)[m] = make_uint4(0u, 0u, 0u, 0u);
+  __syncwarp();
+  uint32_t bs[32];  // bucket << 10 | arrival slot
+#pragma unroll
+  for (int j = 0; j < 32; ++j) {
+    const uint32_t koff = key[j] - kmin, r = 32u * lane + j;
+    uint32_t b, vv;
+    if (!wide) {
+      vv = (koff << 10) | r;
+      b = vv >> shb;
+    } else {
+      b = koff >> (shb - 10u);
+      vv = ((koff & ((1u << (shb - 10u)) - 1u)) << 10) | r;
+    }
+    key[j] = vv;
+    bs[j] = 0;
+    if (full || 32u * j + lane < nvalid) {
+      const uint32_t h = (b & 1u) << 4;
+      const uint32_t old = atomicAdd(&hist[sx(b >> 1)], 1u << h);
+      bs[j] = (b << 10) | ((old >> h) & 0x3FFu);
+    }
+  }
+  __syncwarp();
+  // exclusive scan of the bucket counts; lane l owns buckets 64l..64l+63
+  unsigned long long multi = 0, big = 0;
+  {
+    uint32_t w[32];
+#pragma unroll
+    for (int m = 0; m < 8; ++m) {
+      const uint4 t = *reinterpret_cast<const uint4 *>(hist + qoff(lane, m));
+      w[4 * m] = t.x; w[4 * m + 1] = t.y; w[4 * m + 2] = t.z; w[4 * m + 3] = t.w;
+    }
+    uint32_t tot = 0;
+#pragma unroll
+    for (int k = 0; k < 32; ++k) {
+      const uint32_t c0 = w[k] & 0xFFFFu, c1 = w[k] >> 16;
+      multi |= (unsigned long long)(c0 > 1u) << (2 * k);
+      multi |= (unsigned long long)(c1 > 1u) << (2 * k + 1);
+      big |= (unsigned long long)(c0 > (uint32_t)kEncSmall) << (2 * k);
+      big |= (unsigned long long)(c1 > (uint32_t)kEncSmall) << (2 * k + 1);
+      w[k] = tot | ((tot + c0) << 16);
+      tot += c0 + c1;
+    }
+    uint32_t inc = tot;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t t = __shfl_up_sync(FULL, inc, o);
+      if (lane >= o) inc += t;
+    }
+    const uint32_t b0 = inc - tot, b2 = b0 | (b0 << 16);
+#pragma unroll
+    for (int m = 0; m < 8; ++m)
+      *reinterpret_cast<uint4 *>(hist + qoff(lane, m)) =
+          make_uint4(w[4 * m] + b2, w[4 * m + 1] + b2, w[4 * m + 2] + b2, w[4 * m + 3] + b2);
+  }
+  __syncwarp();
+  // place: bucket start + arrival slot
+#pragma unroll
+  for (int j = 0; j < 32; ++j) {
+    if (full || 32u * j + lane < nvalid) {
+      const uint32_t b = bs[j] >> 10;
+      S[sx(bucket_start(hist, b, nvalid) + (bs[j] & 0x3FFu))] = key[j];
+    }
+  }
+  __syncwarp();
+  // order the multi-point buckets: small ones by their owning lane
+  {
+    unsigned long long sm = multi & ~big;
+    while (sm) {
+      const int k = __ffsll((long long)sm) - 1;
+      sm &= sm - 1;
+      const uint32_t b = 64u * lane + k;
+      const uint32_t st = bucket_start(hist, b, nvalid), en = bucket_start(hist, b + 1, nvalid);
+      for (uint32_t i = st + 1; i < en; ++i) {
+        const uint32_t x = S[sx(i)];
+        uint32_t k2 = i;
+        while (k2 > st) {
+          const uint32_t y = S[sx(k2 - 1)];
+          if (y <= x) break;
+          S[sx(k2)] = y;
+          --k2;
+        }
+        S[sx(k2)] = x;
+      }
+    }
+  }
+  __syncwarp();
+  // large buckets: the whole warp, one at a time
+  {
+    unsigned long long bg = big;
+    for (;;) {
+      const uint32_t who = __ballot_sync(FULL, bg != 0);
+      if (!who) break;
+      const int src = __ffs((int)who) - 1;
+      const unsigned long long lbg = __shfl_sync(FULL, bg, src);
+      const int k = __ffsll((long long)lbg) - 1;
+      if (lane == src) bg &= bg - 1;
+      const uint32_t b = 64u * src + k;
+      const uint32_t st = bucket_start(hist, b, nvalid), en = bucket_start(hist, b + 1, nvalid);
+      warp_bitonic_u32(S, st, en - st, lane);
+    }
+  }
+  __syncwarp();
+
+  // ---- sorted order: this lane's positions 32l..32l+31 ----
+  uint32_t rp[16];  // rank r of positions j and j+16 (16-bit pairs)
+  {
+#pragma unroll
+    for (int m = 0; m < 8; ++m) {
+      const uint4 t = *reinterpret_cast<const uint4 *>(S + qoff(lane, m));
+      key[4 * m] = t.x; key[4 * m + 1] = t.y; key[4 * m + 2] = t.z; key[4 * m + 3] = t.w;
+    }
+#pragma unroll
+    for (int k = 0; k < 16; ++k) rp[k] = (key[k] & 1023u) | ((key[k + 16] & 1023u) << 16);
+    if (wide) {
+      // bucket of every position: max-scan of bucket indices written at the
+      // bucket starts (the count words are done with)
+      uint32_t st2[32];
+#pragma unroll
+      for (int m = 0; m < 8; ++m) {
+        const uint4 t = *reinterpret_cast<const uint4 *>(hist + qoff(lane, m));
+        st2[4 * m] = t.x; st2[4 * m + 1] = t.y; st2[4 * m + 2] = t.z; st2[4 * m + 3] = t.w;
+      }
+      const uint32_t next0 = __shfl_down_sync(FULL, st2[0] & 0xFFFFu, 1);
+      __syncwarp();
+#pragma unroll
+      for (int m = 0; m < 8; ++m) reinterpret_cast<uint4 *>(hist + 32 * lane)[m] = make_uint4(0u, 0u, 0u, 0u);
+      __syncwarp();
+#pragma unroll
+      for (int k = 0; k < 32; ++k) {
+        const uint32_t s0 = st2[k] & 0xFFFFu, s1 = st2[k] >> 16;
+        const uint32_t e1 = k < 31 ? (st2[k + 1] & 0xFFFFu) : (lane < 31 ? next0 : nvalid);
+        if (s1 > s0) hist[sx(s0)] = 64u * lane + 2 * k;
+        if (e1 > s1) hist[sx(s1)] = 64u * lane + 2 * k + 1;
+      }
+      __syncwarp();
+      uint32_t mxb = 0, bpos[32];
+#pragma unroll
+      for (int m = 0; m < 8; ++m) {
+        const uint4 t = *reinterpret_cast<const uint4 *>(hist + qoff(lane, m));
+        mxb = max(mxb, t.x); bpos[4 * m] = mxb;
+        mxb = max(mxb, t.y); bpos[4 * m + 1] = mxb;
+        mxb = max(mxb, t.z); bpos[4 * m + 2] = mxb;
+        mxb = max(mxb, t.w); bpos[4 * m + 3] = mxb;
+      }
+      uint32_t inc = mxb;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t t = __shfl_up_sync(FULL, inc, o);
+        if (lane >= o) inc = max(inc, t);
+      }
+      uint32_t pre = __shfl_up_sync(FULL, inc, 1);
+      if (lane == 0) pre = 0;
+#pragma unroll
+      for (int j = 0; j < 32; ++j) key[j] = kmin + ((max(bpos[j], pre) << (shb - 10u)) | (key[j] >> 10));
+    } else {
+#pragma unroll
+      for (int j = 0; j < 32; ++j) key[j] = kmin + (key[j] >> 10);
+    }
+  }
+  __syncwarp();  // ranked composites and bucket words are done with
+
+  // ---- 3. runs: unique ids, deltas, counts (:222-311) ----
+  uint32_t *const runStart = sw, *const deltaA = sw + kChunk;
+  uint32_t U, dbits, cbits, first;
+  {
+    const uint32_t prevk = __shfl_up_sync(FULL, key[31], 1);
+    uint32_t fm = 0, dm = 0;
+#pragma unroll
+    for (int j = 0; j < 32; ++j) {
+      const uint32_t pos = 32u * lane + j;
+      const uint32_t pk = j ? key[j - 1] : prevk;
+      const bool st = pos < nvalid && (pos == 0 || key[j] != pk);
+      if (st) {
+        fm |= 1u << j;
+        dm = max(dm, pos == 0 ? 0u : bitlen(key[j] - pk));
+      }
+    }
+    const uint32_t cnt = __popc(fm);
+    uint32_t inc = cnt;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t t = __shfl_up_sync(FULL, inc, o);
+      if (lane >= o) inc += t;
+    }
+    U = __shfl_sync(FULL, inc, 31);
+    dbits = warp_max(dm);
+    first = __shfl_sync(FULL, key[0], 0);
+    uint32_t u = inc - cnt;
+#pragma unroll
+    for (int j = 0; j < 32; ++j) {
+      if ((fm >> j) & 1u) {
+        const uint32_t pos = 32u * lane + j;
+        const uint32_t pk = j ? key[j - 1] : prevk;
+        runStart[sx(u)] = pos;
+        deltaA[sx(u)] = pos == 0 ? 0u : key[j] - pk;
+        ++u;
+      }
+    }
+  }
+  __syncwarp();
+  // this lane's runs 32l..32l+31: deltas, and counts as 16-bit pairs
+  uint32_t dl[32], cp[16];
+  {
+#pragma unroll
+    for (int m = 0; m < 8; ++m) {
+      const uint4 t = *reinterpret_cast<const uint4 *>(runStart + qoff(lane, m));
+      const uint4 q = *reinterpret_cast<const uint4 *>(deltaA + qoff(lane, m));
+      key[4 * m] = t.x; key[4 * m + 1] = t.y; key[4 * m + 2] = t.z; key[4 * m + 3] = t.w;
+      dl[4 * m] = q.x; dl[4 * m + 1] = q.y; dl[4 * m + 2] = q.z; dl[4 * m + 3] = q.w;
+    }
+#pragma unroll
+    for (int j = 0; j < 32; ++j) {
+      const bool live = 32u * lane + j < U;
+      key[j] = live ? key[j] : nvalid;
+      dl[j] = live ? dl[j] : 0u;
+    }
+    const uint32_t nx = __shfl_down_sync(FULL, key[0], 1);
+    uint32_t cm = 0;
+#pragma unroll
+    for (int j = 0; j < 32; ++j) {
+      const uint32_t e = j < 31 ? key[j + 1] : (lane < 31 ? nx : nvalid);
+      key[j] = e - key[j];  // run length (0 past the last run)
+      cm = max(cm, key[j]);
+    }
+#pragma unroll
+    for (int k = 0; k < 16; ++k) cp[k] = key[k] | (key[k + 16] << 16);
+    cbits = bitlen(warp_max(cm));
+  }
+  __syncwarp();  // run rows read: the region becomes the payload staging
+
+  // ---- 4. bit planes -> staged payload (:313-411) ----
+  const uint32_t db = section_bytes(U, dbits, Tr::pad), cb = section_bytes(U, cbits, Tr::pad);
+  const uint32_t rb = rel_section_bytes(rbits, Tr::pad);
+  const uint32_t bpp = (U + 7u) >> 3;
+  uint32_t *const stage = sw;
+  put_planes(stage, 0u, dbits, bpp, dl, lane);
+#pragma unroll
+  for (int k = 0; k < 16; ++k) { dl[k] = cp[k] & 0xFFFFu; dl[k + 16] = cp[k] >> 16; }
+  put_planes(stage, db, cbits, bpp, dl, lane);
+  // delta + count sections end below 8 KB: the rank rows are still intact
+#pragma unroll
+  for (int j = 0; j < 32; ++j) {
+    const uint32_t r = (rp[j & 15] >> (16 * (j >> 4))) & 0xFFFFu;
+    dl[j] = 32u * lane + j < nvalid ? relR[sx(r)] : 0xFFFFFFFFu;  // invalid slots (:197)
+  }
+  __syncwarp();
+  put_planes(stage, db + cb, rbits, 0u, dl, lane);
+  {
+    // section padding is zero (the reference leaves it unwritten)
+    uint8_t *stage8 = reinterpret_cast<uint8_t *>(stage);
+    const uint32_t p0 = dbits * bpp + lane, p1 = db + cbits * bpp + lane;
+    if (p0 < db) stage8[p0] = 0;
+    if (p1 < db + cb) stage8[p1] = 0;
+  }
+
+  // meta record (:332-344 / Double :333-345)
+  {
+    uint32_t w = 0;
+    T mv = mm[0];
+#pragma unroll
+    for (int k = 1; k < 6; ++k)
+      if ((is64 ? (lane >> 1) : lane) == k) mv = mm[k];
+    if (!is64) {
+      if (lane < 6) w = __float_as_uint((float)mv);
+      if (lane == 6) w = first;
+      if (lane == 7) w = dbits | (cbits << 16);
+      if (lane == 8) w = rbits | (U << 16);
+    } else {
+      if (lane < 12) {
+        const unsigned long long b = (unsigned long long)__double_as_longlong((double)mv);
+        w = (lane & 1) ? (uint32_t)(b >> 32) : (uint32_t)b;
+      }
+      if (lane == 12) w = first;
+      if (lane == 13) w = 0;
+      if (lane == 14) w = dbits | (cbits << 16);
+      if (lane == 15) w = rbits | (U << 16);
+    }
+    meta_word = w;
+  }
+  return db + cb + rb;
+}
+
+template <typename T, int DIM>
+__global__ void __launch_bounds__(32 * kEncWarps, 4) compress_kernel(const CArgs<T> a) {
+  using Tr = TT<T>;
+  constexpr bool is64 = sizeof(T) == 8;
+  constexpr uint32_t FULL = 0xFFFFFFFFu;
+  extern __shared__ __align__(16) uint32_t enc_smem[];
+  __shared__ EncGroup eg;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  uint32_t *const sw = enc_smem + warp * kEncWords;
+  Control *ctl = a.ctl;
+  if (ld_volatile(reinterpret_cast<const uint32_t *>(&ctl->status)) != 0) return;
+  const uint32_t seg = ctl->seg;
+  const uint32_t sh = (uint32_t)__ffs((int)seg) - 1u, msk = seg - 1u;
+  const T eb = a.eb;
+  const T inv = is64 ? (T)__ddiv_rn(1.0, __dmul_rn(2.0, (double)eb)) : (T)__fdiv_rn(1.0f, __fmul_rn(2.0f, (float)eb));
+  const unsigned long long G = a.G;
+  const unsigned long long pay_base = Tr::hdr + 8ull * G + (unsigned long long)Tr::meta * G;
+
+  if (threadIdx.x == 0) eg.next = atomicAdd(&ctl->chunk_ctr, (uint32_t)kEncWarps);
+  __syncthreads();
+  for (;;) {
+    const unsigned long long gbase = eg.next;
+    if (gbase >= G) break;
+    __syncthreads();  // B0: everyone has the group before it is replaced
+    if (threadIdx.x == 0) eg.next = ld_volatile(&ctl->abort) ? G : atomicAdd(&ctl->chunk_ctr, (uint32_t)kEncWarps);
+    const unsigned long long c = gbase + warp;
+    uint32_t payload = 0, meta_word = 0;
+    if (c < G) payload = encode_chunk<T, DIM>(a, c, sw, seg, sh, msk, inv, meta_word, lane);
+    if (lane == 0) eg.sz[warp] = payload;
+    __syncthreads();  // B1: the group's sizes are known
+    if (warp == 0) {
+      const uint32_t s = lane < kEncWarps ? eg.sz[lane] : 0u;
+      const uint32_t total = __reduce_add_sync(FULL, s);
+      const unsigned long long gid = gbase / kEncWarps;
+      if (lane == 0) publish_aggregate(a.look, gid, total);
+      unsigned long long excl = 0;
+      const bool ok = resolve_prefix(a.look, gid, total, ctl, excl);
+      if (lane == 0) eg.goff = ok ? excl : ~0ull;
+    }
+    __syncthreads();  // B2: the group's stream offset is known
+    const unsigned long long goff = eg.goff;
+    if (c < G && goff != ~0ull) {
+      unsigned long long off = goff;
+      for (int w = 0; w < warp; ++w) off += eg.sz[w];
+      if (lane == 0) reinterpret_cast<unsigned long long *>(a.out + Tr::hdr)[c] = off;  // :1679
+      uint8_t *meta = a.out + Tr::hdr + 8ull * G + (unsigned long long)Tr::meta * c;
+      if (lane < (int)(Tr::meta / 4)) reinterpret_cast<uint32_t *>(meta)[lane] = meta_word;
+      if (c == 0) {
+        // header (:1674-1678; Double :1672-1680)
+        uint32_t *h = reinterpret_cast<uint32_t *>(a.out);
+        if (lane == 0) h[0] = a.dim;
+        if (lane == 1) h[1] = (uint32_t)a.n;
+        if (lane == 2) h[2] = (uint32_t)(a.n >> 32);
+        if (lane == 3) h[3] = Tr::bits;
+        if (!is64) {
+          if (lane == 4) h[4] = __float_as_uint((float)a.eb);
+          if (lane == 5) h[5] = seg;
+        } else {
+          if (lane == 4) h[4] = (uint32_t)__double_as_longlong((double)a.eb);
+          if (lane == 5) h[5] = (uint32_t)((unsigned long long)__double_as_longlong((double)a.eb) >> 32);
+          if (lane == 6) h[6] = seg;
+          if (lane == 7) h[7] = 32u;
+        }
+      }
+      if (pay_base + off + payload > a.out_cap) {
+        if (lane == 0) set_status(ctl, kENOSPACE);
+      } else {
+        uint32_t *dst = reinterpret_cast<uint32_t *>(a.out + pay_base + off);
+        for (uint32_t w = lane; w < payload / 4u; w += 32) dst[w] = sw[w];
+      }
+      if (c == G - 1 && lane == 0) ctl->stream_bytes = pay_base + off + payload;
+    }
+  }
+  rewind_work_counter(ctl);
+}
+
+}  // namespace gpzb
