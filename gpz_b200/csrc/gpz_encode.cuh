@@ -24,13 +24,17 @@
 #pragma once
 
 #include <cfloat>
+#include <type_traits>
 #include "gpz_kernels.cuh"
 
 namespace gpzb {
 
+#ifndef GPZ_ENC_MIN_CTAS
+#define GPZ_ENC_MIN_CTAS 4                // resident CTAs per SM the register budget is sized for
+#endif
 constexpr int kEncWarps = 4;              // chunks (warps) per CTA
 constexpr int kEncBucketBits = 11;        // ranking buckets per chunk: 2048
-constexpr int kEncSmall = 16;             // larger buckets are sorted by the whole warp
+constexpr int kEncSmall = 16;             // buckets of this many points or more are sorted by the whole warp
 constexpr int kEncWords = 3 * kChunk;     // per-warp shared words (12 KB)
 static_assert(kStageBytes <= kEncWords * 4, "payload staging must fit the warp region");
 
@@ -67,6 +71,119 @@ __device__ void warp_bitonic_u32(uint32_t *a, uint32_t lo, uint32_t n, int lane)
       }
       __syncwarp();
     }
+  }
+}
+
+// Batcher's odd-even merge sort network on 32 registers (191 exchanges).
+__host__ __device__ __forceinline__ void oem_sort32(uint32_t (&a)[32]) {
+#pragma unroll
+  for (int p = 1; p < 32; p <<= 1)
+#pragma unroll
+    for (int k = p; k >= 1; k >>= 1)
+#pragma unroll
+      for (int j = k % p; j + k < 32; j += 2 * k)
+#pragma unroll
+        for (int i = 0; i < k; ++i)
+          if (i + j + k < 32 && (i + j) / (2 * p) == (i + j + k) / (2 * p)) {
+            const uint32_t x = a[i + j], y = a[i + j + k];
+            a[i + j] = x < y ? x : y;
+            a[i + j + k] = x < y ? y : x;
+          }
+}
+
+// Merges two ascending halves a[0..15], a[16..31] (bitonic merge: the first
+// stage compares mirrored positions, then half-cleaners).
+__host__ __device__ __forceinline__ void merge_halves32(uint32_t (&a)[32]) {
+#pragma unroll
+  for (int i = 0; i < 16; ++i) {
+    const uint32_t x = a[i], y = a[31 - i];
+    a[i] = x < y ? x : y;
+    a[31 - i] = x < y ? y : x;
+  }
+#pragma unroll
+  for (int s = 8; s >= 1; s >>= 1)
+#pragma unroll
+    for (int i = 0; i < 32; ++i)
+      if ((i & s) == 0) {
+        const uint32_t x = a[i], y = a[i + s];
+        a[i] = x < y ? x : y;
+        a[i + s] = x < y ? y : x;
+      }
+}
+
+// Row <-> column transposes of the warp's 32x32 value matrix through a
+// 1024-word swizzled scratch (row l = lane l's registers).  Column reads and
+// writes touch one row per instruction, so all 32 banks; c[t] is the lane's
+// column offset inside rows with (row & 7) == t.
+__device__ __forceinline__ void column_offsets(uint32_t (&c)[8], int lane) {
+#pragma unroll
+  for (int t = 0; t < 8; ++t) c[t] = ((uint32_t)(((lane >> 2) ^ t) & 7) << 2) + (lane & 3);
+}
+__device__ __forceinline__ void rows_to_columns(uint32_t (&v)[32], uint32_t *tsm, const uint32_t (&c)[8], int lane) {
+#pragma unroll
+  for (int m = 0; m < 8; ++m)
+    *reinterpret_cast<uint4 *>(tsm + qoff(lane, m)) = make_uint4(v[4 * m], v[4 * m + 1], v[4 * m + 2], v[4 * m + 3]);
+  __syncwarp();
+#pragma unroll
+  for (int j = 0; j < 32; ++j) v[j] = tsm[32 * j + c[j & 7]];
+}
+__device__ __forceinline__ void columns_to_rows(uint32_t (&v)[32], uint32_t *tsm, const uint32_t (&c)[8], int lane) {
+#pragma unroll
+  for (int j = 0; j < 32; ++j) tsm[32 * j + c[j & 7]] = v[j];
+  __syncwarp();
+#pragma unroll
+  for (int m = 0; m < 8; ++m) {
+    const uint4 t = *reinterpret_cast<const uint4 *>(tsm + qoff(lane, m));
+    v[4 * m] = t.x; v[4 * m + 1] = t.y; v[4 * m + 2] = t.z; v[4 * m + 3] = t.w;
+  }
+}
+
+__device__ __forceinline__ void cas_up(uint32_t &x, uint32_t &y) {
+  const uint32_t lo = min(x, y);
+  y = max(x, y);
+  x = lo;
+}
+
+// Ascending sort of the warp's 1024 values, lane l holding elements
+// 32l..32l+31 in v[0..31].  Bitonic sort in the variant whose comparators
+// all keep the minimum at the lower index: each merge of size k first pairs
+// mirrored elements (i, i ^ (k-1)), then (i, i + d) for d = k/4 .. 1.  Lanes
+// first sort their rows (odd-even merge network).  For k >= 64 the stages of
+// distance >= 32 run on the transposed matrix (lane L holding elements
+// 32j + L), where distance-d pairs are registers j, j + d/32 and the mirrored
+// pairs are register j ^ (k/32 - 1) of lane 31 - L.
+__device__ __forceinline__ void warp_sort1024(uint32_t (&v)[32], uint32_t *tsm, int lane) {
+  constexpr uint32_t FULL = 0xFFFFFFFFu;
+  uint32_t c[8];
+  column_offsets(c, lane);
+  oem_sort32(v);
+#pragma unroll
+  for (int lk = 6; lk <= 10; ++lk) {
+    rows_to_columns(v, tsm, c, lane);
+    {
+      const int mk = (1 << (lk - 5)) - 1, hb = 1 << (lk - 6);
+#pragma unroll
+      for (int j = 0; j < 32; ++j)
+        if ((j & hb) == 0) {
+          const int jj = j ^ mk;
+          const uint32_t pj = __shfl_xor_sync(FULL, v[jj], 31), pjj = __shfl_xor_sync(FULL, v[j], 31);
+          v[j] = min(v[j], pj);
+          v[jj] = max(v[jj], pjj);
+        }
+    }
+#pragma unroll
+    for (int s = lk - 2; s >= 5; --s) {
+      const int dj = 1 << (s - 5);
+#pragma unroll
+      for (int j = 0; j < 32; ++j)
+        if ((j & dj) == 0) cas_up(v[j], v[j | dj]);
+    }
+    columns_to_rows(v, tsm, c, lane);
+#pragma unroll
+    for (int d = 16; d >= 1; d >>= 1)
+#pragma unroll
+      for (int j = 0; j < 32; ++j)
+        if ((j & d) == 0) cas_up(v[j], v[j | d]);
   }
 }
 
@@ -120,11 +237,44 @@ __device__ __forceinline__ void put_planes(uint32_t *stage, uint32_t pos0, uint3
   }
 }
 
+// The points of one chunk, loaded ahead of encoding: float streams keep all
+// axes in registers (element j of lane l is point 32j + l of the chunk), so a
+// chunk costs one round of loads and the next chunk's loads overlap the
+// current one's placement.  Double streams load one axis at a time.
+template <typename T, int DIM>
+struct ChunkPoints {
+  static constexpr bool kAhead = sizeof(T) == 4;
+  T v[kAhead ? DIM : 1][32];
+  __device__ __forceinline__ void load(const CArgs<T> &a, unsigned long long c, int lane) {
+    if constexpr (kAhead) {
+      c = c < a.G ? c : a.G - 1;  // past the end: reload the last chunk (unused)
+      const unsigned long long base = c * kChunk;
+      const uint32_t nvalid = (uint32_t)min((unsigned long long)kChunk, a.n - base);
+      const T *const X[3] = {a.x, a.y, a.z};
+      if (nvalid == (uint32_t)kChunk) {
+#pragma unroll
+        for (int d = 0; d < DIM; ++d)
+#pragma unroll
+          for (int j = 0; j < 32; ++j) v[d][j] = X[d][base + 32u * j + lane];
+      } else {
+#pragma unroll
+        for (int d = 0; d < DIM; ++d)
+#pragma unroll
+          for (int j = 0; j < 32; ++j) {
+            const uint32_t p = 32u * j + lane;
+            v[d][j] = p < nvalid ? X[d][base + p] : (T)0;
+          }
+      }
+    }
+  }
+};
+
 // Encodes chunk c into the warp's region `sw`; returns the payload bytes and
 // leaves the meta record in meta[] (word k of the record in lane k).
 template <typename T, int DIM>
-__device__ uint32_t encode_chunk(const CArgs<T> &a, unsigned long long c, uint32_t *sw, uint32_t seg, uint32_t sh,
-                                 uint32_t msk, T inv, uint32_t &meta_word, int lane) {
+__device__ __forceinline__ uint32_t encode_chunk(const CArgs<T> &a, unsigned long long c, uint32_t *sw,
+                                                 uint32_t seg, uint32_t sh, uint32_t msk, T inv,
+                                                 ChunkPoints<T, DIM> &pts, uint32_t &meta_word, int lane) {
   using Tr = TT<T>;
   using UO = typename Tr::U;
   constexpr bool is64 = sizeof(T) == 8;
@@ -147,20 +297,26 @@ __device__ uint32_t encode_chunk(const CArgs<T> &a, unsigned long long c, uint32
   uint32_t rmax = 0;
 #pragma unroll
   for (int d = 0; d < DIM; ++d) {
-    T v[32];
-    const T *src = X[d] + base;
+    T vl[ChunkPoints<T, DIM>::kAhead ? 1 : 32];
+    if constexpr (!ChunkPoints<T, DIM>::kAhead) {
+      const T *src = X[d] + base;
 #pragma unroll
-    for (int j = 0; j < 32; ++j) {
-      const uint32_t p = 32u * j + lane;
-      v[j] = (full || p < nvalid) ? src[p] : (T)0;
+      for (int j = 0; j < 32; ++j) {
+        const uint32_t p = 32u * j + lane;
+        vl[j] = (full || p < nvalid) ? src[p] : (T)0;
+      }
     }
+    auto vv_of = [&](int j) -> T {
+      if constexpr (ChunkPoints<T, DIM>::kAhead) return pts.v[d][j];
+      else return vl[j];
+    };
     // fmin / fmax ignore NaN and order -0.0 below +0.0, as the reference's
     // warp reductions do (:122-139)
     const T lim = is64 ? (T)DBL_MAX : (T)FLT_MAX;
     T mn = lim, mx = -lim;
 #pragma unroll
     for (int j = 0; j < 32; ++j)
-      if (full || 32u * j + lane < nvalid) { mn = fmin(mn, v[j]); mx = fmax(mx, v[j]); }
+      if (full || 32u * j + lane < nvalid) { mn = fmin(mn, vv_of(j)); mx = fmax(mx, vv_of(j)); }
     mn = from_ord((UO)~warp_max((UO)~ord_of(mn)));
     mx = from_ord(warp_max(ord_of(mx)));
     mm[d] = mn;
@@ -184,11 +340,11 @@ __device__ uint32_t encode_chunk(const CArgs<T> &a, unsigned long long c, uint32
         const int j = 4 * m + e;
         uint32_t kq, r;
         if constexpr (!is64) {
-          const uint32_t q = __float2uint_rz(__fmaf_rn((float)v[j], (float)inv, (float)nmn));
+          const uint32_t q = __float2uint_rz(__fmaf_rn((float)vv_of(j), (float)inv, (float)nmn));
           kq = q >> sh;
           r = q & msk;
         } else {
-          const unsigned long long q = __double2ull_rz(__fma_rn((double)v[j], (double)inv, (double)nmn));
+          const unsigned long long q = __double2ull_rz(__fma_rn((double)vv_of(j), (double)inv, (double)nmn));
           kq = (uint32_t)(q >> sh);
           r = (uint32_t)(q & msk);
         }
@@ -226,170 +382,177 @@ __device__ uint32_t encode_chunk(const CArgs<T> &a, unsigned long long c, uint32
   // ---- 2. rank the composites (block id - kmin) << 10 | r ----
   const unsigned long long cmax = ((unsigned long long)(kmax - kmin) << 10) | 1023ull;
   const uint32_t cbits_all = bitlen64(cmax);
-  const uint32_t shb = cbits_all > (uint32_t)kEncBucketBits ? cbits_all - kEncBucketBits : 0u;
-  const bool wide = cbits_all > 32u;  // then S keeps the composite's bits below the bucket
-#pragma unroll
-  for (int m = 0; m < 8; ++m) reinterpret_cast<uint4 *>(hist + 32 * lane)[m] = make_uint4(0u, 0u, 0u, 0u);
-  __syncwarp();
-  uint32_t bs[32];  // bucket << 10 | arrival slot
-#pragma unroll
-  for (int j = 0; j < 32; ++j) {
-    const uint32_t koff = key[j] - kmin, r = 32u * lane + j;
-    uint32_t b, vv;
-    if (!wide) {
-      vv = (koff << 10) | r;
-      b = vv >> shb;
-    } else {
-      b = koff >> (shb - 10u);
-      vv = ((koff & ((1u << (shb - 10u)) - 1u)) << 10) | r;
-    }
-    key[j] = vv;
-    bs[j] = 0;
-    if (full || 32u * j + lane < nvalid) {
-      const uint32_t h = (b & 1u) << 4;
-      const uint32_t old = atomicAdd(&hist[sx(b >> 1)], 1u << h);
-      bs[j] = (b << 10) | ((old >> h) & 0x3FFu);
-    }
-  }
-  __syncwarp();
-  // exclusive scan of the bucket counts; lane l owns buckets 64l..64l+63
-  unsigned long long multi = 0, big = 0;
-  {
-    uint32_t w[32];
-#pragma unroll
-    for (int m = 0; m < 8; ++m) {
-      const uint4 t = *reinterpret_cast<const uint4 *>(hist + qoff(lane, m));
-      w[4 * m] = t.x; w[4 * m + 1] = t.y; w[4 * m + 2] = t.z; w[4 * m + 3] = t.w;
-    }
-    uint32_t tot = 0;
-#pragma unroll
-    for (int k = 0; k < 32; ++k) {
-      const uint32_t c0 = w[k] & 0xFFFFu, c1 = w[k] >> 16;
-      multi |= (unsigned long long)(c0 > 1u) << (2 * k);
-      multi |= (unsigned long long)(c1 > 1u) << (2 * k + 1);
-      big |= (unsigned long long)(c0 > (uint32_t)kEncSmall) << (2 * k);
-      big |= (unsigned long long)(c1 > (uint32_t)kEncSmall) << (2 * k + 1);
-      w[k] = tot | ((tot + c0) << 16);
-      tot += c0 + c1;
-    }
-    uint32_t inc = tot;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      const uint32_t t = __shfl_up_sync(FULL, inc, o);
-      if (lane >= o) inc += t;
-    }
-    const uint32_t b0 = inc - tot, b2 = b0 | (b0 << 16);
-#pragma unroll
-    for (int m = 0; m < 8; ++m)
-      *reinterpret_cast<uint4 *>(hist + qoff(lane, m)) =
-          make_uint4(w[4 * m] + b2, w[4 * m + 1] + b2, w[4 * m + 2] + b2, w[4 * m + 3] + b2);
-  }
-  __syncwarp();
-  // place: bucket start + arrival slot
-#pragma unroll
-  for (int j = 0; j < 32; ++j) {
-    if (full || 32u * j + lane < nvalid) {
-      const uint32_t b = bs[j] >> 10;
-      S[sx(bucket_start(hist, b, nvalid) + (bs[j] & 0x3FFu))] = key[j];
-    }
-  }
-  __syncwarp();
-  // order the multi-point buckets: small ones by their owning lane
-  {
-    unsigned long long sm = multi & ~big;
-    while (sm) {
-      const int k = __ffsll((long long)sm) - 1;
-      sm &= sm - 1;
-      const uint32_t b = 64u * lane + k;
-      const uint32_t st = bucket_start(hist, b, nvalid), en = bucket_start(hist, b + 1, nvalid);
-      for (uint32_t i = st + 1; i < en; ++i) {
-        const uint32_t x = S[sx(i)];
-        uint32_t k2 = i;
-        while (k2 > st) {
-          const uint32_t y = S[sx(k2 - 1)];
-          if (y <= x) break;
-          S[sx(k2)] = y;
-          --k2;
-        }
-        S[sx(k2)] = x;
-      }
-    }
-  }
-  __syncwarp();
-  // large buckets: the whole warp, one at a time
-  {
-    unsigned long long bg = big;
-    for (;;) {
-      const uint32_t who = __ballot_sync(FULL, bg != 0);
-      if (!who) break;
-      const int src = __ffs((int)who) - 1;
-      const unsigned long long lbg = __shfl_sync(FULL, bg, src);
-      const int k = __ffsll((long long)lbg) - 1;
-      if (lane == src) bg &= bg - 1;
-      const uint32_t b = 64u * src + k;
-      const uint32_t st = bucket_start(hist, b, nvalid), en = bucket_start(hist, b + 1, nvalid);
-      warp_bitonic_u32(S, st, en - st, lane);
-    }
-  }
-  __syncwarp();
-
-  // ---- sorted order: this lane's positions 32l..32l+31 ----
   uint32_t rp[16];  // rank r of positions j and j+16 (16-bit pairs)
-  {
+  if (cbits_all <= 32u) {
+    // 32-bit composites: sorted in registers; points past the chunk's end
+    // sort last
 #pragma unroll
-    for (int m = 0; m < 8; ++m) {
-      const uint4 t = *reinterpret_cast<const uint4 *>(S + qoff(lane, m));
-      key[4 * m] = t.x; key[4 * m + 1] = t.y; key[4 * m + 2] = t.z; key[4 * m + 3] = t.w;
-    }
+    for (int j = 0; j < 32; ++j)
+      key[j] = (full || 32u * j + lane < nvalid) ? (((key[j] - kmin) << 10) | (32u * lane + j)) : FULL;
+    warp_sort1024(key, hist, lane);
 #pragma unroll
     for (int k = 0; k < 16; ++k) rp[k] = (key[k] & 1023u) | ((key[k + 16] & 1023u) << 16);
-    if (wide) {
-      // bucket of every position: max-scan of bucket indices written at the
-      // bucket starts (the count words are done with)
-      uint32_t st2[32];
 #pragma unroll
+    for (int j = 0; j < 32; ++j) key[j] = kmin + (key[j] >> 10);
+  } else {
+    // wider composites: 2048 buckets on the top bits, S keeps the bits below
+    const uint32_t shb = cbits_all - kEncBucketBits;
+  #pragma unroll
+    for (int m = 0; m < 8; ++m) reinterpret_cast<uint4 *>(hist + 32 * lane)[m] = make_uint4(0u, 0u, 0u, 0u);
+    __syncwarp();
+    uint32_t bs[32];  // bucket << 10 | arrival slot
+    auto count_pass = [&](auto wide_c) {
+      constexpr bool WIDE = decltype(wide_c)::value;
+  #pragma unroll
+      for (int j = 0; j < 32; ++j) {
+        const uint32_t koff = key[j] - kmin, r = 32u * lane + j;
+        uint32_t b, vv;
+        if constexpr (!WIDE) {
+          vv = (koff << 10) | r;
+          b = vv >> shb;
+        } else {
+          b = koff >> (shb - 10u);
+          vv = ((koff & ((1u << (shb - 10u)) - 1u)) << 10) | r;
+        }
+        key[j] = vv;
+        bs[j] = 0;
+        if (full || 32u * j + lane < nvalid) {
+          const uint32_t h = (b & 1u) << 4;
+          const uint32_t old = atomicAdd(&hist[sx(b >> 1)], 1u << h);
+          bs[j] = (b << 10) | ((old >> h) & 0x3FFu);
+        }
+      }
+    };
+    count_pass(std::true_type{});
+    __syncwarp();
+    // exclusive scan of the bucket counts; lane l owns buckets 64l..64l+63
+    uint32_t bigw = 0;  // bit k: a bucket of count word k holds 16 or more points
+    {
+      uint32_t w[32];
+  #pragma unroll
       for (int m = 0; m < 8; ++m) {
         const uint4 t = *reinterpret_cast<const uint4 *>(hist + qoff(lane, m));
-        st2[4 * m] = t.x; st2[4 * m + 1] = t.y; st2[4 * m + 2] = t.z; st2[4 * m + 3] = t.w;
+        w[4 * m] = t.x; w[4 * m + 1] = t.y; w[4 * m + 2] = t.z; w[4 * m + 3] = t.w;
       }
-      const uint32_t next0 = __shfl_down_sync(FULL, st2[0] & 0xFFFFu, 1);
-      __syncwarp();
-#pragma unroll
-      for (int m = 0; m < 8; ++m) reinterpret_cast<uint4 *>(hist + 32 * lane)[m] = make_uint4(0u, 0u, 0u, 0u);
-      __syncwarp();
-#pragma unroll
+      uint32_t tot = 0;
+  #pragma unroll
       for (int k = 0; k < 32; ++k) {
-        const uint32_t s0 = st2[k] & 0xFFFFu, s1 = st2[k] >> 16;
-        const uint32_t e1 = k < 31 ? (st2[k + 1] & 0xFFFFu) : (lane < 31 ? next0 : nvalid);
-        if (s1 > s0) hist[sx(s0)] = 64u * lane + 2 * k;
-        if (e1 > s1) hist[sx(s1)] = 64u * lane + 2 * k + 1;
+        const uint32_t c0 = w[k] & 0xFFFFu;
+        if (w[k] & 0xFFF0FFF0u) bigw |= 1u << k;
+        const uint32_t st = tot | ((tot + c0) << 16);
+        tot += c0 + (w[k] >> 16);
+        w[k] = st;
       }
-      __syncwarp();
-      uint32_t mxb = 0, bpos[32];
-#pragma unroll
-      for (int m = 0; m < 8; ++m) {
-        const uint4 t = *reinterpret_cast<const uint4 *>(hist + qoff(lane, m));
-        mxb = max(mxb, t.x); bpos[4 * m] = mxb;
-        mxb = max(mxb, t.y); bpos[4 * m + 1] = mxb;
-        mxb = max(mxb, t.z); bpos[4 * m + 2] = mxb;
-        mxb = max(mxb, t.w); bpos[4 * m + 3] = mxb;
-      }
-      uint32_t inc = mxb;
-#pragma unroll
+      uint32_t inc = tot;
+  #pragma unroll
       for (int o = 1; o < 32; o <<= 1) {
         const uint32_t t = __shfl_up_sync(FULL, inc, o);
-        if (lane >= o) inc = max(inc, t);
+        if (lane >= o) inc += t;
       }
-      uint32_t pre = __shfl_up_sync(FULL, inc, 1);
-      if (lane == 0) pre = 0;
-#pragma unroll
-      for (int j = 0; j < 32; ++j) key[j] = kmin + ((max(bpos[j], pre) << (shb - 10u)) | (key[j] >> 10));
-    } else {
-#pragma unroll
-      for (int j = 0; j < 32; ++j) key[j] = kmin + (key[j] >> 10);
+      const uint32_t b0 = inc - tot, b2 = b0 | (b0 << 16);
+  #pragma unroll
+      for (int m = 0; m < 8; ++m)
+        *reinterpret_cast<uint4 *>(hist + qoff(lane, m)) =
+            make_uint4(w[4 * m] + b2, w[4 * m + 1] + b2, w[4 * m + 2] + b2, w[4 * m + 3] + b2);
+    }
+    __syncwarp();
+    // place: bucket start + arrival slot; every point now lies inside its
+    // bucket's range of S, and the buckets are in order
+  #pragma unroll
+    for (int j = 0; j < 32; ++j) {
+      if (full || 32u * j + lane < nvalid) {
+        const uint32_t b = bs[j] >> 10;
+        S[sx(bucket_start(hist, b, nvalid) + (bs[j] & 0x3FFu))] = key[j];
+      }
+    }
+    __syncwarp();
+    // buckets of 16 or more points: the whole warp sorts each one
+    while (__any_sync(FULL, bigw != 0)) {
+      const int src = __ffs((int)__ballot_sync(FULL, bigw != 0)) - 1;
+      const int k = __ffs((int)__shfl_sync(FULL, bigw, src)) - 1;
+      if (lane == src) bigw &= bigw - 1;
+  #pragma unroll 1
+      for (uint32_t b = 64u * src + 2 * k; b < 64u * src + 2 * k + 2; ++b) {
+        const uint32_t st = bucket_start(hist, b, nvalid), en = bucket_start(hist, b + 1, nvalid);
+        if (en - st >= (uint32_t)kEncSmall) warp_bitonic_u32(S, st, en - st, lane);
+      }
+    }
+    {
+      // wide composites (S holds the bits below the bucket): each lane orders
+      // its own small buckets by insertion
+  #pragma unroll 1
+      for (uint32_t b = 64u * lane; b < 64u * lane + 64u; ++b) {
+        const uint32_t st = bucket_start(hist, b, nvalid), en = bucket_start(hist, b + 1, nvalid);
+        if (en - st < 2u || en - st >= (uint32_t)kEncSmall) continue;
+        for (uint32_t i = st + 1; i < en; ++i) {
+          const uint32_t x = S[sx(i)];
+          uint32_t k2 = i;
+          while (k2 > st) {
+            const uint32_t y = S[sx(k2 - 1)];
+            if (y <= x) break;
+            S[sx(k2)] = y;
+            --k2;
+          }
+          S[sx(k2)] = x;
+        }
+      }
+    }
+    __syncwarp();
+
+    // sorted order: this lane's positions 32l..32l+31
+    {
+  #pragma unroll
+      for (int m = 0; m < 8; ++m) {
+        const uint4 t = *reinterpret_cast<const uint4 *>(S + qoff(lane, m));
+        key[4 * m] = t.x; key[4 * m + 1] = t.y; key[4 * m + 2] = t.z; key[4 * m + 3] = t.w;
+      }
+  #pragma unroll
+      for (int k = 0; k < 16; ++k) rp[k] = (key[k] & 1023u) | ((key[k + 16] & 1023u) << 16);
+      {
+        // bucket of every position: max-scan of bucket indices written at the
+        // bucket starts (the count words are done with)
+        uint32_t st2[32];
+  #pragma unroll
+        for (int m = 0; m < 8; ++m) {
+          const uint4 t = *reinterpret_cast<const uint4 *>(hist + qoff(lane, m));
+          st2[4 * m] = t.x; st2[4 * m + 1] = t.y; st2[4 * m + 2] = t.z; st2[4 * m + 3] = t.w;
+        }
+        const uint32_t next0 = __shfl_down_sync(FULL, st2[0] & 0xFFFFu, 1);
+        __syncwarp();
+  #pragma unroll
+        for (int m = 0; m < 8; ++m) reinterpret_cast<uint4 *>(hist + 32 * lane)[m] = make_uint4(0u, 0u, 0u, 0u);
+        __syncwarp();
+  #pragma unroll
+        for (int k = 0; k < 32; ++k) {
+          const uint32_t s0 = st2[k] & 0xFFFFu, s1 = st2[k] >> 16;
+          const uint32_t e1 = k < 31 ? (st2[k + 1] & 0xFFFFu) : (lane < 31 ? next0 : nvalid);
+          if (s1 > s0) hist[sx(s0)] = 64u * lane + 2 * k;
+          if (e1 > s1) hist[sx(s1)] = 64u * lane + 2 * k + 1;
+        }
+        __syncwarp();
+        uint32_t mxb = 0, bpos[32];
+  #pragma unroll
+        for (int m = 0; m < 8; ++m) {
+          const uint4 t = *reinterpret_cast<const uint4 *>(hist + qoff(lane, m));
+          mxb = max(mxb, t.x); bpos[4 * m] = mxb;
+          mxb = max(mxb, t.y); bpos[4 * m + 1] = mxb;
+          mxb = max(mxb, t.z); bpos[4 * m + 2] = mxb;
+          mxb = max(mxb, t.w); bpos[4 * m + 3] = mxb;
+        }
+        uint32_t inc = mxb;
+  #pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+          const uint32_t t = __shfl_up_sync(FULL, inc, o);
+          if (lane >= o) inc = max(inc, t);
+        }
+        uint32_t pre = __shfl_up_sync(FULL, inc, 1);
+        if (lane == 0) pre = 0;
+  #pragma unroll
+        for (int j = 0; j < 32; ++j) key[j] = kmin + ((max(bpos[j], pre) << (shb - 10u)) | (key[j] >> 10));
+      }
     }
   }
-  __syncwarp();  // ranked composites and bucket words are done with
+  __syncwarp();  // ranking scratch is done with
 
   // ---- 3. runs: unique ids, deltas, counts (:222-311) ----
   uint32_t *const runStart = sw, *const deltaA = sw + kChunk;
@@ -513,7 +676,7 @@ __device__ uint32_t encode_chunk(const CArgs<T> &a, unsigned long long c, uint32
 }
 
 template <typename T, int DIM>
-__global__ void __launch_bounds__(32 * kEncWarps, 4) compress_kernel(const CArgs<T> a) {
+__global__ void __launch_bounds__(32 * kEncWarps, GPZ_ENC_MIN_CTAS) compress_kernel(const CArgs<T> a) {
   using Tr = TT<T>;
   constexpr bool is64 = sizeof(T) == 8;
   constexpr uint32_t FULL = 0xFFFFFFFFu;
@@ -532,6 +695,8 @@ __global__ void __launch_bounds__(32 * kEncWarps, 4) compress_kernel(const CArgs
 
   if (threadIdx.x == 0) eg.next = atomicAdd(&ctl->chunk_ctr, (uint32_t)kEncWarps);
   __syncthreads();
+  ChunkPoints<T, DIM> pts;
+  pts.load(a, eg.next + warp, lane);
   for (;;) {
     const unsigned long long gbase = eg.next;
     if (gbase >= G) break;
@@ -539,9 +704,10 @@ __global__ void __launch_bounds__(32 * kEncWarps, 4) compress_kernel(const CArgs
     if (threadIdx.x == 0) eg.next = ld_volatile(&ctl->abort) ? G : atomicAdd(&ctl->chunk_ctr, (uint32_t)kEncWarps);
     const unsigned long long c = gbase + warp;
     uint32_t payload = 0, meta_word = 0;
-    if (c < G) payload = encode_chunk<T, DIM>(a, c, sw, seg, sh, msk, inv, meta_word, lane);
+    if (c < G) payload = encode_chunk<T, DIM>(a, c, sw, seg, sh, msk, inv, pts, meta_word, lane);
     if (lane == 0) eg.sz[warp] = payload;
-    __syncthreads();  // B1: the group's sizes are known
+    __syncthreads();  // B1: the group's sizes are known (and the next group's id)
+    pts.load(a, eg.next + warp, lane);  // in flight during the look-back and copy-out
     if (warp == 0) {
       const uint32_t s = lane < kEncWarps ? eg.sz[lane] : 0u;
       const uint32_t total = __reduce_add_sync(FULL, s);

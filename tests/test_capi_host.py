@@ -63,10 +63,14 @@ def test_host_argument_errors_without_gpu():
     assert rc == gz.GPZ_EINVAL
 
 
-def test_fast_divider_exact(tmp_path):
-    exe = tmp_path / "fastdiv"
-    subprocess.run(["nvcc", "-std=c++17", "-O2", "-gencode", "arch=compute_100a,code=sm_100a", "-I", os.path.join(ROOT, "gpz_b200", "csrc"),
-                    "-o", str(exe), os.path.join(ROOT, "tests", "host", "fastdiv_check.cu")], check=True)
+@pytest.mark.parametrize("check", ["fastdiv_check", "transpose_check", "network_check"])
+def test_device_helpers_on_host(tmp_path, check):
+    """Exact dividers, bit-plane transposes and register sorting networks of the
+    kernels, compiled for the host and checked against plain arithmetic."""
+    exe = tmp_path / check
+    subprocess.run(["nvcc", "-std=c++17", "-O2", "-gencode", "arch=compute_100a,code=sm_100a",
+                    "-I", os.path.join(ROOT, "gpz_b200", "csrc"), "-I", os.path.join(ROOT, "include"),
+                    "-o", str(exe), os.path.join(ROOT, "tests", "host", check + ".cu")], check=True)
     out = subprocess.run([str(exe)], capture_output=True, text=True)
     assert out.returncode == 0, out.stdout + out.stderr
     assert "bad=0" in out.stdout
