@@ -19,7 +19,7 @@
 //      them through shared memory so lane l holds runs 32l..32l+31;
 //   4. transposes deltas, counts and relative positions into bit planes in
 //      registers and assembles the payload in its shared region.
-// The 4 warps of a CTA take 4 consecutive chunks together; one decoupled
+// The 8 warps of a CTA take 8 consecutive chunks together; one decoupled
 // look-back per group places the group's payloads in the stream.
 #pragma once
 
@@ -30,9 +30,12 @@
 namespace gpzb {
 
 #ifndef GPZ_ENC_MIN_CTAS
-#define GPZ_ENC_MIN_CTAS 4                // resident CTAs per SM the register budget is sized for
+#define GPZ_ENC_MIN_CTAS 2                // resident CTAs per SM the register budget is sized for
 #endif
-constexpr int kEncWarps = 4;              // chunks (warps) per CTA
+#ifndef GPZ_ENC_WARPS
+#define GPZ_ENC_WARPS 8
+#endif
+constexpr int kEncWarps = GPZ_ENC_WARPS;  // chunks (warps) per CTA
 constexpr int kEncBucketBits = 11;        // ranking buckets per chunk: 2048
 constexpr int kEncSmall = 16;             // buckets of this many points or more are sorted by the whole warp
 constexpr int kEncWords = 3 * kChunk;     // per-warp shared words (12 KB)
@@ -144,16 +147,22 @@ __device__ __forceinline__ void cas_up(uint32_t &x, uint32_t &y) {
   x = lo;
 }
 
-// Ascending sort of the warp's 1024 values, lane l holding elements
-// 32l..32l+31 in v[0..31].  Bitonic sort in the variant whose comparators
+// Ascending sort of the warp's 1024 values held in the swizzled rows `rows`
+// (lane l: elements 32l..32l+31), in place; tsm is a second 1024-word scratch.  Bitonic sort in the variant whose comparators
 // all keep the minimum at the lower index: each merge of size k first pairs
 // mirrored elements (i, i ^ (k-1)), then (i, i + d) for d = k/4 .. 1.  Lanes
 // first sort their rows (odd-even merge network).  For k >= 64 the stages of
 // distance >= 32 run on the transposed matrix (lane L holding elements
 // 32j + L), where distance-d pairs are registers j, j + d/32 and the mirrored
 // pairs are register j ^ (k/32 - 1) of lane 31 - L.
-__device__ __forceinline__ void warp_sort1024(uint32_t (&v)[32], uint32_t *tsm, int lane) {
+__device__ __noinline__ void warp_sort1024_rows(uint32_t *rows, uint32_t *tsm, int lane) {
   constexpr uint32_t FULL = 0xFFFFFFFFu;
+  uint32_t v[32];
+#pragma unroll
+  for (int m = 0; m < 8; ++m) {
+    const uint4 t = *reinterpret_cast<const uint4 *>(rows + qoff(lane, m));
+    v[4 * m] = t.x; v[4 * m + 1] = t.y; v[4 * m + 2] = t.z; v[4 * m + 3] = t.w;
+  }
   uint32_t c[8];
   column_offsets(c, lane);
   oem_sort32(v);
@@ -185,6 +194,9 @@ __device__ __forceinline__ void warp_sort1024(uint32_t (&v)[32], uint32_t *tsm, 
       for (int j = 0; j < 32; ++j)
         if ((j & d) == 0) cas_up(v[j], v[j | d]);
   }
+#pragma unroll
+  for (int m = 0; m < 8; ++m)
+    *reinterpret_cast<uint4 *>(rows + qoff(lane, m)) = make_uint4(v[4 * m], v[4 * m + 1], v[4 * m + 2], v[4 * m + 3]);
 }
 
 // Start of bucket b (b = 2048 gives the number of ranked points).
@@ -235,6 +247,190 @@ __device__ __forceinline__ void put_planes(uint32_t *stage, uint32_t pos0, uint3
     for (int b = 0; b < 32; ++b)
       if ((uint32_t)b < nb) put(b, v[b]);
   }
+}
+
+// Ranks a chunk whose composites (block id - kmin) << 10 | r need more than
+// 32 bits: 2048 buckets on the top bits (shared-atomic counts, placement by
+// bucket start + arrival slot), S keeping the bits below the bucket; buckets
+// of 2..15 points ordered by their owning lane, larger ones by the warp.  On
+// entry S's row l holds lane l's block ids; on exit S's row l holds the
+// sorted block ids of positions 32l..32l+31 and the first 16 words of hist's
+// row l the ranks r of positions j, j+16 as 16-bit pairs.
+__device__ __noinline__ void rank_wide(uint32_t *sw, uint32_t kmin, uint32_t cbits_all, uint32_t nvalid, int lane) {
+  constexpr uint32_t FULL = 0xFFFFFFFFu;
+  uint32_t *const S = sw, *const hist = sw + kChunk;
+  const bool full = nvalid == (uint32_t)kChunk;
+  uint32_t key[32], rp[16];
+#pragma unroll
+  for (int m = 0; m < 8; ++m) {
+    const uint4 t = *reinterpret_cast<const uint4 *>(S + qoff(lane, m));
+    key[4 * m] = t.x; key[4 * m + 1] = t.y; key[4 * m + 2] = t.z; key[4 * m + 3] = t.w;
+  }
+  __syncwarp();
+  // wider composites: 2048 buckets on the top bits, S keeps the bits below
+  const uint32_t shb = cbits_all - kEncBucketBits;
+#pragma unroll
+  for (int m = 0; m < 8; ++m) reinterpret_cast<uint4 *>(hist + 32 * lane)[m] = make_uint4(0u, 0u, 0u, 0u);
+  __syncwarp();
+  uint32_t bs[32];  // bucket << 10 | arrival slot
+  auto count_pass = [&](auto wide_c) {
+    constexpr bool WIDE = decltype(wide_c)::value;
+#pragma unroll
+    for (int j = 0; j < 32; ++j) {
+      const uint32_t koff = key[j] - kmin, r = 32u * lane + j;
+      uint32_t b, vv;
+      if constexpr (!WIDE) {
+        vv = (koff << 10) | r;
+        b = vv >> shb;
+      } else {
+        b = koff >> (shb - 10u);
+        vv = ((koff & ((1u << (shb - 10u)) - 1u)) << 10) | r;
+      }
+      key[j] = vv;
+      bs[j] = 0;
+      if (full || 32u * j + lane < nvalid) {
+        const uint32_t h = (b & 1u) << 4;
+        const uint32_t old = atomicAdd(&hist[sx(b >> 1)], 1u << h);
+        bs[j] = (b << 10) | ((old >> h) & 0x3FFu);
+      }
+    }
+  };
+  count_pass(std::true_type{});
+  __syncwarp();
+  // exclusive scan of the bucket counts; lane l owns buckets 64l..64l+63
+  uint32_t bigw = 0;  // bit k: a bucket of count word k holds 16 or more points
+  {
+    uint32_t w[32];
+#pragma unroll
+    for (int m = 0; m < 8; ++m) {
+      const uint4 t = *reinterpret_cast<const uint4 *>(hist + qoff(lane, m));
+      w[4 * m] = t.x; w[4 * m + 1] = t.y; w[4 * m + 2] = t.z; w[4 * m + 3] = t.w;
+    }
+    uint32_t tot = 0;
+#pragma unroll
+    for (int k = 0; k < 32; ++k) {
+      const uint32_t c0 = w[k] & 0xFFFFu;
+      if (w[k] & 0xFFF0FFF0u) bigw |= 1u << k;
+      const uint32_t st = tot | ((tot + c0) << 16);
+      tot += c0 + (w[k] >> 16);
+      w[k] = st;
+    }
+    uint32_t inc = tot;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t t = __shfl_up_sync(FULL, inc, o);
+      if (lane >= o) inc += t;
+    }
+    const uint32_t b0 = inc - tot, b2 = b0 | (b0 << 16);
+#pragma unroll
+    for (int m = 0; m < 8; ++m)
+      *reinterpret_cast<uint4 *>(hist + qoff(lane, m)) =
+          make_uint4(w[4 * m] + b2, w[4 * m + 1] + b2, w[4 * m + 2] + b2, w[4 * m + 3] + b2);
+  }
+  __syncwarp();
+  // place: bucket start + arrival slot; every point now lies inside its
+  // bucket's range of S, and the buckets are in order
+#pragma unroll
+  for (int j = 0; j < 32; ++j) {
+    if (full || 32u * j + lane < nvalid) {
+      const uint32_t b = bs[j] >> 10;
+      S[sx(bucket_start(hist, b, nvalid) + (bs[j] & 0x3FFu))] = key[j];
+    }
+  }
+  __syncwarp();
+  // buckets of 16 or more points: the whole warp sorts each one
+  while (__any_sync(FULL, bigw != 0)) {
+    const int src = __ffs((int)__ballot_sync(FULL, bigw != 0)) - 1;
+    const int k = __ffs((int)__shfl_sync(FULL, bigw, src)) - 1;
+    if (lane == src) bigw &= bigw - 1;
+#pragma unroll 1
+    for (uint32_t b = 64u * src + 2 * k; b < 64u * src + 2 * k + 2; ++b) {
+      const uint32_t st = bucket_start(hist, b, nvalid), en = bucket_start(hist, b + 1, nvalid);
+      if (en - st >= (uint32_t)kEncSmall) warp_bitonic_u32(S, st, en - st, lane);
+    }
+  }
+  {
+    // wide composites (S holds the bits below the bucket): each lane orders
+    // its own small buckets by insertion
+#pragma unroll 1
+    for (uint32_t b = 64u * lane; b < 64u * lane + 64u; ++b) {
+      const uint32_t st = bucket_start(hist, b, nvalid), en = bucket_start(hist, b + 1, nvalid);
+      if (en - st < 2u || en - st >= (uint32_t)kEncSmall) continue;
+      for (uint32_t i = st + 1; i < en; ++i) {
+        const uint32_t x = S[sx(i)];
+        uint32_t k2 = i;
+        while (k2 > st) {
+          const uint32_t y = S[sx(k2 - 1)];
+          if (y <= x) break;
+          S[sx(k2)] = y;
+          --k2;
+        }
+        S[sx(k2)] = x;
+      }
+    }
+  }
+  __syncwarp();
+
+  // sorted order: this lane's positions 32l..32l+31
+  {
+#pragma unroll
+    for (int m = 0; m < 8; ++m) {
+      const uint4 t = *reinterpret_cast<const uint4 *>(S + qoff(lane, m));
+      key[4 * m] = t.x; key[4 * m + 1] = t.y; key[4 * m + 2] = t.z; key[4 * m + 3] = t.w;
+    }
+#pragma unroll
+    for (int k = 0; k < 16; ++k) rp[k] = (key[k] & 1023u) | ((key[k + 16] & 1023u) << 16);
+    {
+      // bucket of every position: max-scan of bucket indices written at the
+      // bucket starts (the count words are done with)
+      uint32_t st2[32];
+#pragma unroll
+      for (int m = 0; m < 8; ++m) {
+        const uint4 t = *reinterpret_cast<const uint4 *>(hist + qoff(lane, m));
+        st2[4 * m] = t.x; st2[4 * m + 1] = t.y; st2[4 * m + 2] = t.z; st2[4 * m + 3] = t.w;
+      }
+      const uint32_t next0 = __shfl_down_sync(FULL, st2[0] & 0xFFFFu, 1);
+      __syncwarp();
+#pragma unroll
+      for (int m = 0; m < 8; ++m) reinterpret_cast<uint4 *>(hist + 32 * lane)[m] = make_uint4(0u, 0u, 0u, 0u);
+      __syncwarp();
+#pragma unroll
+      for (int k = 0; k < 32; ++k) {
+        const uint32_t s0 = st2[k] & 0xFFFFu, s1 = st2[k] >> 16;
+        const uint32_t e1 = k < 31 ? (st2[k + 1] & 0xFFFFu) : (lane < 31 ? next0 : nvalid);
+        if (s1 > s0) hist[sx(s0)] = 64u * lane + 2 * k;
+        if (e1 > s1) hist[sx(s1)] = 64u * lane + 2 * k + 1;
+      }
+      __syncwarp();
+      uint32_t mxb = 0, bpos[32];
+#pragma unroll
+      for (int m = 0; m < 8; ++m) {
+        const uint4 t = *reinterpret_cast<const uint4 *>(hist + qoff(lane, m));
+        mxb = max(mxb, t.x); bpos[4 * m] = mxb;
+        mxb = max(mxb, t.y); bpos[4 * m + 1] = mxb;
+        mxb = max(mxb, t.z); bpos[4 * m + 2] = mxb;
+        mxb = max(mxb, t.w); bpos[4 * m + 3] = mxb;
+      }
+      uint32_t inc = mxb;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t t = __shfl_up_sync(FULL, inc, o);
+        if (lane >= o) inc = max(inc, t);
+      }
+      uint32_t pre = __shfl_up_sync(FULL, inc, 1);
+      if (lane == 0) pre = 0;
+#pragma unroll
+      for (int j = 0; j < 32; ++j) key[j] = kmin + ((max(bpos[j], pre) << (shb - 10u)) | (key[j] >> 10));
+    }
+  }
+  __syncwarp();
+#pragma unroll
+  for (int m = 0; m < 8; ++m)
+    *reinterpret_cast<uint4 *>(S + qoff(lane, m)) = make_uint4(key[4 * m], key[4 * m + 1], key[4 * m + 2], key[4 * m + 3]);
+#pragma unroll
+  for (int m = 0; m < 4; ++m)
+    *reinterpret_cast<uint4 *>(hist + qoff(lane, m)) = make_uint4(rp[4 * m], rp[4 * m + 1], rp[4 * m + 2], rp[4 * m + 3]);
+  __syncwarp();
 }
 
 // The points of one chunk, loaded ahead of encoding: float streams keep all
@@ -367,6 +563,21 @@ __device__ __forceinline__ uint32_t encode_chunk(const CArgs<T> &a, unsigned lon
     }
   }
   if (DIM == 2) { mm[2] = (T)0; mm[5] = (T)0; }  // 2D meta carries z = 0 (:518, :521)
+  // this lane's word of the meta record's min/max part (:332-344 / Double
+  // :333-345), taken now so the six values need no registers later
+  uint32_t mword = 0;
+  {
+    T mv = mm[0];
+#pragma unroll
+    for (int k = 1; k < 6; ++k)
+      if ((is64 ? (lane >> 1) : lane) == k) mv = mm[k];
+    if (!is64) {
+      mword = __float_as_uint((float)mv);
+    } else {
+      const unsigned long long b = (unsigned long long)__double_as_longlong((double)mv);
+      mword = (lane & 1) ? (uint32_t)(b >> 32) : (uint32_t)b;
+    }
+  }
   if (lane == 0 && bound > 0x7FFFFFFFull) a.ctl->id_overflow = 1u;
   uint32_t kmin = FULL, kmax = 0;
 #pragma unroll
@@ -384,172 +595,44 @@ __device__ __forceinline__ uint32_t encode_chunk(const CArgs<T> &a, unsigned lon
   const uint32_t cbits_all = bitlen64(cmax);
   uint32_t rp[16];  // rank r of positions j and j+16 (16-bit pairs)
   if (cbits_all <= 32u) {
-    // 32-bit composites: sorted in registers; points past the chunk's end
-    // sort last
+    // 32-bit composites: one data-independent warp sort; points past the
+    // chunk's end hold the maximum and sort last
 #pragma unroll
-    for (int j = 0; j < 32; ++j)
-      key[j] = (full || 32u * j + lane < nvalid) ? (((key[j] - kmin) << 10) | (32u * lane + j)) : FULL;
-    warp_sort1024(key, hist, lane);
+    for (int m = 0; m < 8; ++m) {
+      uint32_t cv[4];
+#pragma unroll
+      for (int e = 0; e < 4; ++e) {
+        const int j = 4 * m + e;
+        cv[e] = (full || 32u * j + lane < nvalid) ? (((key[j] - kmin) << 10) | (32u * lane + j)) : FULL;
+      }
+      *reinterpret_cast<uint4 *>(S + qoff(lane, m)) = make_uint4(cv[0], cv[1], cv[2], cv[3]);
+    }
+    warp_sort1024_rows(S, hist, lane);
+#pragma unroll
+    for (int m = 0; m < 8; ++m) {
+      const uint4 t = *reinterpret_cast<const uint4 *>(S + qoff(lane, m));
+      key[4 * m] = t.x; key[4 * m + 1] = t.y; key[4 * m + 2] = t.z; key[4 * m + 3] = t.w;
+    }
 #pragma unroll
     for (int k = 0; k < 16; ++k) rp[k] = (key[k] & 1023u) | ((key[k + 16] & 1023u) << 16);
 #pragma unroll
     for (int j = 0; j < 32; ++j) key[j] = kmin + (key[j] >> 10);
   } else {
-    // wider composites: 2048 buckets on the top bits, S keeps the bits below
-    const uint32_t shb = cbits_all - kEncBucketBits;
-  #pragma unroll
-    for (int m = 0; m < 8; ++m) reinterpret_cast<uint4 *>(hist + 32 * lane)[m] = make_uint4(0u, 0u, 0u, 0u);
-    __syncwarp();
-    uint32_t bs[32];  // bucket << 10 | arrival slot
-    auto count_pass = [&](auto wide_c) {
-      constexpr bool WIDE = decltype(wide_c)::value;
-  #pragma unroll
-      for (int j = 0; j < 32; ++j) {
-        const uint32_t koff = key[j] - kmin, r = 32u * lane + j;
-        uint32_t b, vv;
-        if constexpr (!WIDE) {
-          vv = (koff << 10) | r;
-          b = vv >> shb;
-        } else {
-          b = koff >> (shb - 10u);
-          vv = ((koff & ((1u << (shb - 10u)) - 1u)) << 10) | r;
-        }
-        key[j] = vv;
-        bs[j] = 0;
-        if (full || 32u * j + lane < nvalid) {
-          const uint32_t h = (b & 1u) << 4;
-          const uint32_t old = atomicAdd(&hist[sx(b >> 1)], 1u << h);
-          bs[j] = (b << 10) | ((old >> h) & 0x3FFu);
-        }
-      }
-    };
-    count_pass(std::true_type{});
-    __syncwarp();
-    // exclusive scan of the bucket counts; lane l owns buckets 64l..64l+63
-    uint32_t bigw = 0;  // bit k: a bucket of count word k holds 16 or more points
-    {
-      uint32_t w[32];
-  #pragma unroll
-      for (int m = 0; m < 8; ++m) {
-        const uint4 t = *reinterpret_cast<const uint4 *>(hist + qoff(lane, m));
-        w[4 * m] = t.x; w[4 * m + 1] = t.y; w[4 * m + 2] = t.z; w[4 * m + 3] = t.w;
-      }
-      uint32_t tot = 0;
-  #pragma unroll
-      for (int k = 0; k < 32; ++k) {
-        const uint32_t c0 = w[k] & 0xFFFFu;
-        if (w[k] & 0xFFF0FFF0u) bigw |= 1u << k;
-        const uint32_t st = tot | ((tot + c0) << 16);
-        tot += c0 + (w[k] >> 16);
-        w[k] = st;
-      }
-      uint32_t inc = tot;
-  #pragma unroll
-      for (int o = 1; o < 32; o <<= 1) {
-        const uint32_t t = __shfl_up_sync(FULL, inc, o);
-        if (lane >= o) inc += t;
-      }
-      const uint32_t b0 = inc - tot, b2 = b0 | (b0 << 16);
-  #pragma unroll
-      for (int m = 0; m < 8; ++m)
-        *reinterpret_cast<uint4 *>(hist + qoff(lane, m)) =
-            make_uint4(w[4 * m] + b2, w[4 * m + 1] + b2, w[4 * m + 2] + b2, w[4 * m + 3] + b2);
+    // wider composites (rare): the bucket path, outside the hot path's
+    // register budget; block ids in and results out through S and hist rows
+#pragma unroll
+    for (int m = 0; m < 8; ++m)
+      *reinterpret_cast<uint4 *>(S + qoff(lane, m)) = make_uint4(key[4 * m], key[4 * m + 1], key[4 * m + 2], key[4 * m + 3]);
+    rank_wide(sw, kmin, cbits_all, nvalid, lane);
+#pragma unroll
+    for (int m = 0; m < 8; ++m) {
+      const uint4 t = *reinterpret_cast<const uint4 *>(S + qoff(lane, m));
+      key[4 * m] = t.x; key[4 * m + 1] = t.y; key[4 * m + 2] = t.z; key[4 * m + 3] = t.w;
     }
-    __syncwarp();
-    // place: bucket start + arrival slot; every point now lies inside its
-    // bucket's range of S, and the buckets are in order
-  #pragma unroll
-    for (int j = 0; j < 32; ++j) {
-      if (full || 32u * j + lane < nvalid) {
-        const uint32_t b = bs[j] >> 10;
-        S[sx(bucket_start(hist, b, nvalid) + (bs[j] & 0x3FFu))] = key[j];
-      }
-    }
-    __syncwarp();
-    // buckets of 16 or more points: the whole warp sorts each one
-    while (__any_sync(FULL, bigw != 0)) {
-      const int src = __ffs((int)__ballot_sync(FULL, bigw != 0)) - 1;
-      const int k = __ffs((int)__shfl_sync(FULL, bigw, src)) - 1;
-      if (lane == src) bigw &= bigw - 1;
-  #pragma unroll 1
-      for (uint32_t b = 64u * src + 2 * k; b < 64u * src + 2 * k + 2; ++b) {
-        const uint32_t st = bucket_start(hist, b, nvalid), en = bucket_start(hist, b + 1, nvalid);
-        if (en - st >= (uint32_t)kEncSmall) warp_bitonic_u32(S, st, en - st, lane);
-      }
-    }
-    {
-      // wide composites (S holds the bits below the bucket): each lane orders
-      // its own small buckets by insertion
-  #pragma unroll 1
-      for (uint32_t b = 64u * lane; b < 64u * lane + 64u; ++b) {
-        const uint32_t st = bucket_start(hist, b, nvalid), en = bucket_start(hist, b + 1, nvalid);
-        if (en - st < 2u || en - st >= (uint32_t)kEncSmall) continue;
-        for (uint32_t i = st + 1; i < en; ++i) {
-          const uint32_t x = S[sx(i)];
-          uint32_t k2 = i;
-          while (k2 > st) {
-            const uint32_t y = S[sx(k2 - 1)];
-            if (y <= x) break;
-            S[sx(k2)] = y;
-            --k2;
-          }
-          S[sx(k2)] = x;
-        }
-      }
-    }
-    __syncwarp();
-
-    // sorted order: this lane's positions 32l..32l+31
-    {
-  #pragma unroll
-      for (int m = 0; m < 8; ++m) {
-        const uint4 t = *reinterpret_cast<const uint4 *>(S + qoff(lane, m));
-        key[4 * m] = t.x; key[4 * m + 1] = t.y; key[4 * m + 2] = t.z; key[4 * m + 3] = t.w;
-      }
-  #pragma unroll
-      for (int k = 0; k < 16; ++k) rp[k] = (key[k] & 1023u) | ((key[k + 16] & 1023u) << 16);
-      {
-        // bucket of every position: max-scan of bucket indices written at the
-        // bucket starts (the count words are done with)
-        uint32_t st2[32];
-  #pragma unroll
-        for (int m = 0; m < 8; ++m) {
-          const uint4 t = *reinterpret_cast<const uint4 *>(hist + qoff(lane, m));
-          st2[4 * m] = t.x; st2[4 * m + 1] = t.y; st2[4 * m + 2] = t.z; st2[4 * m + 3] = t.w;
-        }
-        const uint32_t next0 = __shfl_down_sync(FULL, st2[0] & 0xFFFFu, 1);
-        __syncwarp();
-  #pragma unroll
-        for (int m = 0; m < 8; ++m) reinterpret_cast<uint4 *>(hist + 32 * lane)[m] = make_uint4(0u, 0u, 0u, 0u);
-        __syncwarp();
-  #pragma unroll
-        for (int k = 0; k < 32; ++k) {
-          const uint32_t s0 = st2[k] & 0xFFFFu, s1 = st2[k] >> 16;
-          const uint32_t e1 = k < 31 ? (st2[k + 1] & 0xFFFFu) : (lane < 31 ? next0 : nvalid);
-          if (s1 > s0) hist[sx(s0)] = 64u * lane + 2 * k;
-          if (e1 > s1) hist[sx(s1)] = 64u * lane + 2 * k + 1;
-        }
-        __syncwarp();
-        uint32_t mxb = 0, bpos[32];
-  #pragma unroll
-        for (int m = 0; m < 8; ++m) {
-          const uint4 t = *reinterpret_cast<const uint4 *>(hist + qoff(lane, m));
-          mxb = max(mxb, t.x); bpos[4 * m] = mxb;
-          mxb = max(mxb, t.y); bpos[4 * m + 1] = mxb;
-          mxb = max(mxb, t.z); bpos[4 * m + 2] = mxb;
-          mxb = max(mxb, t.w); bpos[4 * m + 3] = mxb;
-        }
-        uint32_t inc = mxb;
-  #pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-          const uint32_t t = __shfl_up_sync(FULL, inc, o);
-          if (lane >= o) inc = max(inc, t);
-        }
-        uint32_t pre = __shfl_up_sync(FULL, inc, 1);
-        if (lane == 0) pre = 0;
-  #pragma unroll
-        for (int j = 0; j < 32; ++j) key[j] = kmin + ((max(bpos[j], pre) << (shb - 10u)) | (key[j] >> 10));
-      }
+#pragma unroll
+    for (int m = 0; m < 4; ++m) {
+      const uint4 t = *reinterpret_cast<const uint4 *>(hist + qoff(lane, m));
+      rp[4 * m] = t.x; rp[4 * m + 1] = t.y; rp[4 * m + 2] = t.z; rp[4 * m + 3] = t.w;
     }
   }
   __syncwarp();  // ranking scratch is done with
@@ -651,20 +734,13 @@ __device__ __forceinline__ uint32_t encode_chunk(const CArgs<T> &a, unsigned lon
   // meta record (:332-344 / Double :333-345)
   {
     uint32_t w = 0;
-    T mv = mm[0];
-#pragma unroll
-    for (int k = 1; k < 6; ++k)
-      if ((is64 ? (lane >> 1) : lane) == k) mv = mm[k];
     if (!is64) {
-      if (lane < 6) w = __float_as_uint((float)mv);
+      if (lane < 6) w = mword;
       if (lane == 6) w = first;
       if (lane == 7) w = dbits | (cbits << 16);
       if (lane == 8) w = rbits | (U << 16);
     } else {
-      if (lane < 12) {
-        const unsigned long long b = (unsigned long long)__double_as_longlong((double)mv);
-        w = (lane & 1) ? (uint32_t)(b >> 32) : (uint32_t)b;
-      }
+      if (lane < 12) w = mword;
       if (lane == 12) w = first;
       if (lane == 13) w = 0;
       if (lane == 14) w = dbits | (cbits << 16);
