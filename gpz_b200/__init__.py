@@ -70,6 +70,9 @@ SIGNATURES = {
     "gpz_compress_noalloc_max_points": (_U64, []),
     "gpz_compress_noalloc": (ctypes.c_int, [ctypes.POINTER(Params), _VP, _VP, _VP, _VP, _U64,
                                             ctypes.POINTER(Result), _VP]),
+    "gpz_aos_to_soa": (ctypes.c_int, [_U32, _U32, _U64, _VP, _VP, _VP, _VP, _VP]),
+    "gpz_soa_to_aos": (ctypes.c_int, [_U32, _U32, _U64, _VP, _VP, _VP, _VP, _VP]),
+    "gpz_stream_size": (ctypes.c_int, [_VP, _U64, ctypes.POINTER(_U64), _VP]),
 }
 
 _lib = None

@@ -132,6 +132,47 @@ int decompress_t(const void *d_stream, uint64_t stream_bytes, uint32_t dim, void
 
 }  // namespace
 
+// AoS <-> SoA for the file path (reference host loops load_file_to_soa_xyz /
+// write_xyz_to_aos_file, include/utils.cuh:83-180).
+template <typename T, int DIM>
+__global__ void __launch_bounds__(256) aos_to_soa_kernel(const T *__restrict__ aos, T *__restrict__ x,
+                                                         T *__restrict__ y, T *__restrict__ z, uint64_t n) {
+  const uint64_t step = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += step) {
+    const T *p = aos + DIM * i;
+    x[i] = p[0];
+    y[i] = p[1];
+    z[i] = DIM == 3 ? p[2] : (T)0;
+  }
+}
+template <typename T, int DIM>
+__global__ void __launch_bounds__(256) soa_to_aos_kernel(const T *__restrict__ x, const T *__restrict__ y,
+                                                         const T *__restrict__ z, T *__restrict__ aos, uint64_t n) {
+  const uint64_t step = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += step) {
+    T *p = aos + DIM * i;
+    p[0] = x[i];
+    p[1] = y[i];
+    if (DIM == 3) p[2] = z[i];
+  }
+}
+
+template <typename T>
+int aos_soa(bool to_soa, uint32_t dim, uint64_t n, const void *aos, const void *x, const void *y, const void *z,
+            cudaStream_t st) {
+  if (n == 0) return GPZ_OK;
+  const unsigned grid = (unsigned)std::min<uint64_t>((n + 255) / 256, (uint64_t)num_sms() * 8);
+  T *X = (T *)x, *Y = (T *)y, *Z = (T *)z, *A = (T *)aos;
+  if (to_soa) {
+    if (dim == 3) aos_to_soa_kernel<T, 3><<<grid, 256, 0, st>>>(A, X, Y, Z, n);
+    else aos_to_soa_kernel<T, 2><<<grid, 256, 0, st>>>(A, X, Y, Z, n);
+  } else {
+    if (dim == 3) soa_to_aos_kernel<T, 3><<<grid, 256, 0, st>>>(X, Y, Z, A, n);
+    else soa_to_aos_kernel<T, 2><<<grid, 256, 0, st>>>(X, Y, Z, A, n);
+  }
+  return cuda_status(cudaGetLastError());
+}
+
 extern "C" {
 
 const char *gpz_version(void) { return "gpz_b200 0.1 (sm_100a)"; }
@@ -265,6 +306,69 @@ int gpz_rel_to_abs(uint32_t float_bits, uint32_t dim, uint64_t n, const void *d_
   if (h_eb) *h_eb = h.out_eb;
   if (h_minmax6)
     for (int k = 0; k < 6; ++k) h_minmax6[k] = h.out_mm[k];
+  return GPZ_OK;
+}
+
+int gpz_aos_to_soa(uint32_t float_bits, uint32_t dim, uint64_t n, const void *d_aos, void *d_x, void *d_y, void *d_z,
+                   void *stream) {
+  if ((float_bits != 32 && float_bits != 64) || (dim != 2 && dim != 3) || (n && (!d_aos || !d_x || !d_y || !d_z)))
+    return GPZ_EINVAL;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  return float_bits == 32 ? aos_soa<float>(true, dim, n, d_aos, d_x, d_y, d_z, st)
+                          : aos_soa<double>(true, dim, n, d_aos, d_x, d_y, d_z, st);
+}
+
+int gpz_soa_to_aos(uint32_t float_bits, uint32_t dim, uint64_t n, const void *d_x, const void *d_y, const void *d_z,
+                   void *d_aos, void *stream) {
+  if ((float_bits != 32 && float_bits != 64) || (dim != 2 && dim != 3) ||
+      (n && (!d_aos || !d_x || !d_y || (dim == 3 && !d_z))))
+    return GPZ_EINVAL;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  return float_bits == 32 ? aos_soa<float>(false, dim, n, d_aos, d_x, d_y, d_z, st)
+                          : aos_soa<double>(false, dim, n, d_aos, d_x, d_y, d_z, st);
+}
+
+int gpz_stream_size(const void *d_stream, uint64_t cap, uint64_t *bytes, void *stream) {
+  if (!d_stream || !bytes) return GPZ_EINVAL;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  const uint8_t *s = static_cast<const uint8_t *>(d_stream);
+  auto fetch = [&](void *dst, uint64_t off, uint64_t len) -> int {
+    if (off > cap || len > cap - off) return GPZ_ESTREAM;
+    if (cudaMemcpyAsync(dst, s + off, len, cudaMemcpyDeviceToHost, st) != cudaSuccess) return GPZ_ECUDA;
+    return cudaStreamSynchronize(st) == cudaSuccess ? GPZ_OK : GPZ_ECUDA;
+  };
+  uint8_t h[32] = {0};
+  int rc = fetch(h, 0, 24);
+  if (rc != GPZ_OK) return rc;
+  uint32_t bits = 0;
+  uint64_t n = 0;
+  memcpy(&n, h + 4, 8);
+  memcpy(&bits, h + 12, 4);
+  if ((bits != 32 && bits != 64) || n == 0) return GPZ_ESTREAM;
+  const uint64_t hdr = bits == 32 ? TT<float>::hdr : TT<double>::hdr;
+  const uint64_t meta = bits == 32 ? TT<float>::meta : TT<double>::meta;
+  const uint32_t pad = bits == 32 ? TT<float>::pad : TT<double>::pad;
+  const uint64_t G = chunks(n);
+  if (G > (UINT64_MAX - hdr) / (8 + meta)) return GPZ_ESTREAM;
+  const uint64_t pay_base = hdr + G * (8 + meta);
+  uint64_t off = 0;
+  uint8_t m[64] = {0};
+  if ((rc = fetch(&off, hdr + 8 * (G - 1), 8)) != GPZ_OK) return rc;
+  if ((rc = fetch(m, hdr + 8 * G + meta * (G - 1), meta)) != GPZ_OK) return rc;
+  uint32_t dbits, cbits, rbits, U;
+  if (bits == 32) {
+    uint16_t f[4];
+    memcpy(f, m + TT<float>::u16_at, 8);
+    dbits = f[0]; cbits = f[1]; rbits = f[2]; U = f[3];
+  } else {
+    uint16_t f[4];
+    memcpy(f, m + TT<double>::u16_at, 8);
+    dbits = f[0]; cbits = f[1]; rbits = f[2]; U = f[3];
+  }
+  if (dbits > 32 || cbits > 32 || rbits > 32) return GPZ_ESTREAM;
+  const uint64_t pl = (uint64_t)section_bytes(U, dbits, pad) + section_bytes(U, cbits, pad) + rel_section_bytes(rbits, pad);
+  if (off > UINT64_MAX - pay_base - pl || pay_base + off + pl > cap) return GPZ_ESTREAM;
+  *bytes = pay_base + off + pl;
   return GPZ_OK;
 }
 

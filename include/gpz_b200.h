@@ -174,6 +174,27 @@ int gpz_compress_noalloc(const gpz_params *params, const void *d_x, const void *
                          const void *d_z, void *d_out, uint64_t out_capacity,
                          gpz_result *result, void *stream);
 
+/* ---- file I/O helpers -----------------------------------------------------------
+ * AoS <-> SoA on the device, for the CLI's file path (the reference does this
+ * with host loops, load_file_to_soa_xyz / write_xyz_to_aos_file,
+ * include/utils.cuh:83-180).  d_aos holds n points of `dim` interleaved
+ * values (x, y[, z]); gpz_aos_to_soa writes zeros to d_z for dim == 2, as the
+ * reference loader does; gpz_soa_to_aos ignores d_z for dim == 2.
+ * Enqueued on `stream`, not synchronised. */
+int gpz_aos_to_soa(uint32_t float_bits, uint32_t dim, uint64_t n, const void *d_aos, void *d_x,
+                   void *d_y, void *d_z, void *stream);
+int gpz_soa_to_aos(uint32_t float_bits, uint32_t dim, uint64_t n, const void *d_x, const void *d_y,
+                   const void *d_z, void *d_aos, void *stream);
+
+/* Total size in bytes of a compressed stream held on the device, from its
+ * header, last offset-table entry and last meta record (three small copies;
+ * synchronises `stream`).  `cap` is the number of bytes readable at
+ * d_stream; GPZ_ESTREAM if the stream does not fit in it.  No counterpart in
+ * the reference, whose decompress takes no size (ICudaCompressor::decompress,
+ * include/ICudaCompressor.cuh:13-14); the C++ drop-in uses it to bound the
+ * stream it validates. */
+int gpz_stream_size(const void *d_stream, uint64_t cap, uint64_t *bytes, void *stream);
+
 /* Library version string. */
 const char *gpz_version(void);
 
