@@ -25,6 +25,7 @@ LIB_PATH = os.path.join(HERE, "libgpz_b200.so")
 
 GPZ_OK, GPZ_EINVAL, GPZ_ESEG, GPZ_ESTREAM, GPZ_ENOSPACE, GPZ_ECUDA, GPZ_ETIMEOUT, GPZ_ENOTSUP, GPZ_ELIMIT = range(9)
 GPZ_FLAG_SAFE31 = 1
+GPZ_FLAG_SEG_FIXED = 2
 ERRORS = {1: "EINVAL", 2: "ESEG", 3: "ESTREAM", 4: "ENOSPACE", 5: "ECUDA", 6: "ETIMEOUT", 7: "ENOTSUP", 8: "ELIMIT"}
 
 
@@ -73,6 +74,12 @@ SIGNATURES = {
     "gpz_aos_to_soa": (ctypes.c_int, [_U32, _U32, _U64, _VP, _VP, _VP, _VP, _VP]),
     "gpz_soa_to_aos": (ctypes.c_int, [_U32, _U32, _U64, _VP, _VP, _VP, _VP, _VP]),
     "gpz_stream_size": (ctypes.c_int, [_VP, _U64, ctypes.POINTER(_U64), _VP]),
+    "gpz_sample_minmax": (ctypes.c_int, [_U32, _U32, _U64, _U64, _U64, _VP, _VP, _VP, _VP, _U64,
+                                         ctypes.POINTER(_U64), _VP]),
+    "gpz_decide_seg": (ctypes.c_int, [_U32, _U32, ctypes.POINTER(_U64), _U32, ctypes.c_int32, ctypes.c_double,
+                                      ctypes.c_double, _U32, ctypes.POINTER(_U32), ctypes.POINTER(_U32)]),
+    "gpz_rel_abs_from_minmax": (ctypes.c_int, [_U32, ctypes.POINTER(ctypes.c_double), ctypes.c_double,
+                                               ctypes.POINTER(ctypes.c_double)]),
 }
 
 _lib = None

@@ -60,8 +60,13 @@ int compress_t(const gpz_params *p, const void *d_x, const void *d_y, const void
   const T eb = (T)p->eb;
   const T rel = (T)p->rel_eb;
   const T *x = static_cast<const T *>(d_x), *y = static_cast<const T *>(d_y), *z = static_cast<const T *>(d_z);
-  seg_sample_kernel<T><<<128, 256, 0, st>>>(x, y, p->dim == 3 ? z : y, p->n, p->dim, p->seg_size, p->rel_mode, rel,
-                                            eb, (p->flags & GPZ_FLAG_SAFE31) ? 1 : 0, ctl);
+  if (p->flags & GPZ_FLAG_SEG_FIXED) {
+    if (p->seg_size == 0) return GPZ_EINVAL;
+    set_seg_kernel<<<1, 1, 0, st>>>(ctl, p->seg_size);
+  } else {
+    seg_sample_kernel<T><<<128, 256, 0, st>>>(x, y, p->dim == 3 ? z : y, p->n, p->dim, p->seg_size, p->rel_mode, rel,
+                                              eb, (p->flags & GPZ_FLAG_SAFE31) ? 1 : 0, ctl);
+  }
   CArgs<T> a;
   a.x = x; a.y = y; a.z = p->dim == 3 ? z : y;
   a.out = static_cast<uint8_t *>(d_out);
@@ -326,6 +331,70 @@ int gpz_soa_to_aos(uint32_t float_bits, uint32_t dim, uint64_t n, const void *d_
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   return float_bits == 32 ? aos_soa<float>(false, dim, n, d_aos, d_x, d_y, d_z, st)
                           : aos_soa<double>(false, dim, n, d_aos, d_x, d_y, d_z, st);
+}
+
+int gpz_sample_minmax(uint32_t float_bits, uint32_t dim, uint64_t n, uint64_t begin, uint64_t count, const void *d_x,
+                      const void *d_y, const void *d_z, void *d_scratch, uint64_t scratch_bytes, uint64_t *h_acc6,
+                      void *stream) {
+  if ((float_bits != 32 && float_bits != 64) || (dim != 2 && dim != 3) || !d_scratch || !h_acc6 || n == 0 ||
+      begin > n || count > n - begin || (count && (!d_x || !d_y || (dim == 3 && !d_z))))
+    return GPZ_EINVAL;
+  if (scratch_bytes < kCtlBytes) return GPZ_ENOSPACE;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  Control *ctl = static_cast<Control *>(d_scratch);
+  if (cudaMemsetAsync(d_scratch, 0, kCtlBytes, st) != cudaSuccess) return GPZ_ECUDA;
+  if (float_bits == 32) {
+    const float *x = (const float *)d_x, *y = (const float *)d_y, *z = (const float *)d_z;
+    seg_sample_shard_kernel<float><<<128, 256, 0, st>>>(x, y, dim == 3 ? z : y, n, begin, count, dim, ctl);
+  } else {
+    const double *x = (const double *)d_x, *y = (const double *)d_y, *z = (const double *)d_z;
+    seg_sample_shard_kernel<double><<<128, 256, 0, st>>>(x, y, dim == 3 ? z : y, n, begin, count, dim, ctl);
+  }
+  if (cudaGetLastError() != cudaSuccess) return GPZ_ECUDA;
+  if (cudaMemcpyAsync(h_acc6, &ctl->mm[0], 6 * sizeof(uint64_t), cudaMemcpyDeviceToHost, st) != cudaSuccess)
+    return GPZ_ECUDA;
+  return cuda_status(cudaStreamSynchronize(st));
+}
+
+int gpz_decide_seg(uint32_t float_bits, uint32_t dim, const uint64_t *acc6, uint32_t seg_in, int32_t rel_mode,
+                   double rel_eb, double eb, uint32_t flags, uint32_t *seg, uint32_t *adjusted) {
+  if ((float_bits != 32 && float_bits != 64) || (dim != 2 && dim != 3) || !acc6 || !seg || !adjusted)
+    return GPZ_EINVAL;
+  SegDecision sd;
+  const int safe31 = (flags & GPZ_FLAG_SAFE31) ? 1 : 0;
+  if (float_bits == 32) {
+    float mm[6] = {0, 0, 0, 0, 0, 0};
+    for (uint32_t d = 0; d < dim; ++d) {
+      mm[d] = from_ord((uint32_t)~(uint32_t)acc6[2 * d]);
+      mm[3 + d] = from_ord((uint32_t)acc6[2 * d + 1]);
+    }
+    sd = decide_seg<float>(mm, dim, seg_in, rel_mode, (float)rel_eb, (float)eb, safe31);
+  } else {
+    double mm[6] = {0, 0, 0, 0, 0, 0};
+    for (uint32_t d = 0; d < dim; ++d) {
+      mm[d] = from_ord((unsigned long long)~acc6[2 * d]);
+      mm[3 + d] = from_ord((unsigned long long)acc6[2 * d + 1]);
+    }
+    sd = decide_seg<double>(mm, dim, seg_in, rel_mode, rel_eb, eb, safe31);
+  }
+  if (sd.status != kOK) return sd.status;
+  *seg = sd.seg;
+  *adjusted = sd.adjusted;
+  return GPZ_OK;
+}
+
+int gpz_rel_abs_from_minmax(uint32_t float_bits, const double *minmax6, double rel, double *eb) {
+  if ((float_bits != 32 && float_bits != 64) || !minmax6 || !eb) return GPZ_EINVAL;
+  if (float_bits == 32) {
+    // convertRelEb<float> (src/main.cpp:35-55), as rel_to_abs_kernel evaluates it
+    const float xr = (float)minmax6[3] - (float)minmax6[0], yr = (float)minmax6[4] - (float)minmax6[1];
+    const float zr = (float)minmax6[5] - (float)minmax6[2];
+    *eb = (double)(fmaxf(fmaxf(xr, yr), zr) * (float)rel);
+  } else {
+    const double xr = minmax6[3] - minmax6[0], yr = minmax6[4] - minmax6[1], zr = minmax6[5] - minmax6[2];
+    *eb = fmax(fmax(xr, yr), zr) * rel;
+  }
+  return GPZ_OK;
 }
 
 int gpz_stream_size(const void *d_stream, uint64_t cap, uint64_t *bytes, void *stream) {

@@ -9,6 +9,7 @@
 #pragma once
 
 #include <cstdint>
+#include <cstring>
 #include <cuda_runtime.h>
 
 namespace gpzb {
@@ -83,19 +84,39 @@ __device__ __forceinline__ void set_status(Control *ctl, int code) {
 // Ordered-integer views of floats: a < b  <=>  ord(a) < ord(b), with -0.0
 // below +0.0, matching FMNMX on the GPU.  NaNs are filtered by the callers.
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ uint32_t ord_of(float f) {
-  uint32_t u = __float_as_uint(f);
+__host__ __device__ __forceinline__ uint32_t f32_bits(float f) {
+  uint32_t u;
+  memcpy(&u, &f, 4);
+  return u;
+}
+__host__ __device__ __forceinline__ float bits_f32(uint32_t u) {
+  float f;
+  memcpy(&f, &u, 4);
+  return f;
+}
+__host__ __device__ __forceinline__ unsigned long long f64_bits(double f) {
+  unsigned long long u;
+  memcpy(&u, &f, 8);
+  return u;
+}
+__host__ __device__ __forceinline__ double bits_f64(unsigned long long u) {
+  double f;
+  memcpy(&f, &u, 8);
+  return f;
+}
+__host__ __device__ __forceinline__ uint32_t ord_of(float f) {
+  const uint32_t u = f32_bits(f);
   return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
 }
-__device__ __forceinline__ float from_ord(uint32_t o) {
-  return __uint_as_float((o & 0x80000000u) ? (o & 0x7FFFFFFFu) : ~o);
+__host__ __device__ __forceinline__ float from_ord(uint32_t o) {
+  return bits_f32((o & 0x80000000u) ? (o & 0x7FFFFFFFu) : ~o);
 }
-__device__ __forceinline__ unsigned long long ord_of(double f) {
-  unsigned long long u = (unsigned long long)__double_as_longlong(f);
+__host__ __device__ __forceinline__ unsigned long long ord_of(double f) {
+  const unsigned long long u = f64_bits(f);
   return (u >> 63) ? ~u : (u | 0x8000000000000000ull);
 }
-__device__ __forceinline__ double from_ord(unsigned long long o) {
-  return __longlong_as_double((long long)((o >> 63) ? (o & 0x7FFFFFFFFFFFFFFFull) : ~o));
+__host__ __device__ __forceinline__ double from_ord(unsigned long long o) {
+  return bits_f64((o >> 63) ? (o & 0x7FFFFFFFFFFFFFFFull) : ~o);
 }
 
 // Warp-wide max of 32/64-bit unsigned values (REDUX on sm_80+).

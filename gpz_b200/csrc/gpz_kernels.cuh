@@ -16,83 +16,166 @@ namespace gpzb {
 // ===========================================================================
 // Automatic segment size (computeSegSize).
 // ===========================================================================
-// Host arithmetic of computeSegSize (src/cudaWarpCompress.cu:1488-1554),
-// evaluated on the device with explicitly rounded operations so no
-// contraction can differ from the reference's host build.
-__device__ void seg_decide(const float mm[6], uint32_t dim, uint32_t seg_in, int rel_mode,
-                           float rel_eb, float eb, int safe31, Control *ctl) {
-  const float dx = __fsub_rn(mm[3], mm[0]), dy = __fsub_rn(mm[4], mm[1]), dz = __fsub_rn(mm[5], mm[2]);
-  const float mean = __fdiv_rn(__fadd_rn(__fadd_rn(dx, dy), dz), 3.0f);
-  const float ex = __fsub_rn(dx, mean), ey = __fsub_rn(dy, mean), ez = __fsub_rn(dz, mean);
-  float var = __fadd_rn(__fadd_rn(__fmul_rn(ex, ex), __fmul_rn(ey, ey)), __fmul_rn(ez, ez));
-  var = __fdiv_rn(var, dim == 3 ? 3.0f : 2.0f);  // the float 2D path divides by 2 (:1503)
-  const float ratio = __fdiv_rn(__fsqrt_rn(var), mean);
-  const float maxr = fmaxf(fmaxf(dx, dy), dz);
+// Correctly rounded scalar operations, the same on the device and on the host
+// (the host build uses plain IEEE operations with contraction off).
+template <typename T> struct Rn;
+template <> struct Rn<float> {
+  __host__ __device__ static float add(float a, float b) {
+#ifdef __CUDA_ARCH__
+    return __fadd_rn(a, b);
+#else
+    return a + b;
+#endif
+  }
+  __host__ __device__ static float sub(float a, float b) {
+#ifdef __CUDA_ARCH__
+    return __fsub_rn(a, b);
+#else
+    return a - b;
+#endif
+  }
+  __host__ __device__ static float mul(float a, float b) {
+#ifdef __CUDA_ARCH__
+    return __fmul_rn(a, b);
+#else
+    return a * b;
+#endif
+  }
+  __host__ __device__ static float div(float a, float b) {
+#ifdef __CUDA_ARCH__
+    return __fdiv_rn(a, b);
+#else
+    return a / b;
+#endif
+  }
+  __host__ __device__ static float sqrt(float a) {
+#ifdef __CUDA_ARCH__
+    return __fsqrt_rn(a);
+#else
+    return sqrtf(a);
+#endif
+  }
+  __host__ __device__ static float from_u32(uint32_t v) {
+#ifdef __CUDA_ARCH__
+    return __uint2float_rn(v);
+#else
+    return (float)v;
+#endif
+  }
+  // truncation with saturation (cvt.rzi.sat.u64), NaN -> 0
+  __host__ __device__ static unsigned long long to_u64_rz(float v) {
+#ifdef __CUDA_ARCH__
+    return __float2ull_rz(v);
+#else
+    if (!(v > 0.0f)) return 0ull;
+    if (v >= 18446744073709551616.0f) return ~0ull;
+    return (unsigned long long)v;
+#endif
+  }
+};
+template <> struct Rn<double> {
+  __host__ __device__ static double add(double a, double b) {
+#ifdef __CUDA_ARCH__
+    return __dadd_rn(a, b);
+#else
+    return a + b;
+#endif
+  }
+  __host__ __device__ static double sub(double a, double b) {
+#ifdef __CUDA_ARCH__
+    return __dsub_rn(a, b);
+#else
+    return a - b;
+#endif
+  }
+  __host__ __device__ static double mul(double a, double b) {
+#ifdef __CUDA_ARCH__
+    return __dmul_rn(a, b);
+#else
+    return a * b;
+#endif
+  }
+  __host__ __device__ static double div(double a, double b) {
+#ifdef __CUDA_ARCH__
+    return __ddiv_rn(a, b);
+#else
+    return a / b;
+#endif
+  }
+  __host__ __device__ static double sqrt(double a) {
+#ifdef __CUDA_ARCH__
+    return __dsqrt_rn(a);
+#else
+    return ::sqrt(a);
+#endif
+  }
+  __host__ __device__ static double from_u32(uint32_t v) {
+#ifdef __CUDA_ARCH__
+    return __uint2double_rn(v);
+#else
+    return (double)v;
+#endif
+  }
+  __host__ __device__ static unsigned long long to_u64_rz(double v) {
+#ifdef __CUDA_ARCH__
+    return __double2ull_rz(v);
+#else
+    if (!(v > 0.0)) return 0ull;
+    if (v >= 18446744073709551616.0) return ~0ull;
+    return (unsigned long long)v;
+#endif
+  }
+};
+
+// Outcome of the automatic segment-size rules.
+struct SegDecision {
+  int status;         // kOK, kEINVAL (no segment size in abs mode) or kESEG
+  uint32_t seg, adjusted;
+};
+
+// Host arithmetic of computeSegSize (src/cudaWarpCompress.cu:1488-1554; double
+// twin src/cudaWarpCompressDouble.cu:1488-1553) on the sampled per-axis
+// min/max mm = (x, y, z minima, x, y, z maxima).  float: the 2D variance
+// divides by 2 (:1503) and seg doubles (<= 11 times) while the block count
+// would exceed UINT32_MAX; double: variance divides by 3 and the reference's
+// guard compares with UINT64_MAX and never fires.  With safe31 both double
+// until every id fits 31 bits.  Evaluated the same on the device (sampling
+// kernel) and on the host (sharded compress).
+template <typename T>
+__host__ __device__ SegDecision decide_seg(const T mm[6], uint32_t dim, uint32_t seg_in, int rel_mode, T rel_eb, T eb,
+                                           int safe31) {
+  using R = Rn<T>;
+  constexpr bool is64 = sizeof(T) == 8;
+  const T dx = R::sub(mm[3], mm[0]), dy = R::sub(mm[4], mm[1]), dz = R::sub(mm[5], mm[2]);
+  const T mean = R::div(R::add(R::add(dx, dy), dz), (T)3);
+  const T ex = R::sub(dx, mean), ey = R::sub(dy, mean), ez = R::sub(dz, mean);
+  T var = R::add(R::add(R::mul(ex, ex), R::mul(ey, ey)), R::mul(ez, ez));
+  var = R::div(var, (!is64 && dim == 2) ? (T)2 : (T)3);
+  const T ratio = R::div(R::sqrt(var), mean);
+  const T maxr3 = is64 ? (T)fmax(fmax((double)dx, (double)dy), (double)dz) : (T)fmaxf(fmaxf((float)dx, (float)dy), (float)dz);
   uint32_t seg = seg_in;
   if (seg == 0 && rel_mode) {
-    if (ratio < 0.1f) seg = ((double)rel_eb <= 1e-4) ? 32u : 2u;
+    if (ratio < (T)0.1f) seg = ((double)rel_eb <= 1e-4) ? 32u : 2u;
     else seg = ((double)rel_eb <= 1e-4) ? 4u : 1u;
   }
-  if (seg == 0) { set_status(ctl, kEINVAL); return; }
+  if (seg == 0) return {kEINVAL, 0u, 0u};
+  const bool guard = !is64 || safe31;
+  if (!guard) return {kOK, seg, 0u};
   const unsigned long long limit = safe31 ? 0x7FFFFFFFull : 0xFFFFFFFFull;
   auto total = [&](uint32_t s) {
-    const unsigned long long mb =
-        __float2ull_rz(ceilf(__fdiv_rn(maxr, __fmul_rn(__uint2float_rn(2u * s), eb)))) + 1ull;
+    const T q = R::div(maxr3, R::mul(R::from_u32(2u * s), eb));
+    const T c = is64 ? (T)::ceil((double)q) : (T)::ceilf((float)q);
+    const unsigned long long mb = R::to_u64_rz(c) + 1ull;
     return dim == 3 ? mb * mb * mb : mb * mb;
   };
-  uint32_t adj = 0;
-  if (total(seg) > limit) {
-    uint32_t t = seg;
-    for (int i = 0; i < 11; ++i) {
-      t *= 2u;
-      if (total(t) <= limit) break;
-    }
-    if (t > 1024u) { set_status(ctl, kESEG); return; }
-    seg = t;
-    adj = 1;
+  if (total(seg) <= limit) return {kOK, seg, 0u};
+  uint32_t t = seg;
+  for (int i = 0; i < 11; ++i) {
+    t *= 2u;
+    if (total(t) <= limit) break;
   }
-  ctl->seg = seg;
-  ctl->adjusted = adj;
-}
-
-// Double twin (src/cudaWarpCompressDouble.cu:1488-1553): variance divides by 3
-// for 2D too, and the reference's overflow guard compares with UINT64_MAX and
-// never fires; only the 31-bit extension adjusts.
-__device__ void seg_decide(const double mm[6], uint32_t dim, uint32_t seg_in, int rel_mode,
-                           double rel_eb, double eb, int safe31, Control *ctl) {
-  const double dx = __dsub_rn(mm[3], mm[0]), dy = __dsub_rn(mm[4], mm[1]), dz = __dsub_rn(mm[5], mm[2]);
-  const double mean = __ddiv_rn(__dadd_rn(__dadd_rn(dx, dy), dz), 3.0);
-  const double ex = __dsub_rn(dx, mean), ey = __dsub_rn(dy, mean), ez = __dsub_rn(dz, mean);
-  double var = __dadd_rn(__dadd_rn(__dmul_rn(ex, ex), __dmul_rn(ey, ey)), __dmul_rn(ez, ez));
-  var = __ddiv_rn(var, 3.0);
-  const double ratio = __ddiv_rn(__dsqrt_rn(var), mean);
-  const double maxr = fmax(fmax(dx, dy), dz);
-  uint32_t seg = seg_in;
-  if (seg == 0 && rel_mode) {
-    if (ratio < (double)0.1f) seg = (rel_eb <= 1e-4) ? 32u : 2u;
-    else seg = (rel_eb <= 1e-4) ? 4u : 1u;
-  }
-  if (seg == 0) { set_status(ctl, kEINVAL); return; }
-  uint32_t adj = 0;
-  if (safe31) {
-    auto total = [&](uint32_t s) {
-      const unsigned long long mb =
-          __double2ull_rz(ceil(__ddiv_rn(maxr, __dmul_rn(__uint2double_rn(2u * s), eb)))) + 1ull;
-      return dim == 3 ? mb * mb * mb : mb * mb;
-    };
-    if (total(seg) > 0x7FFFFFFFull) {
-      uint32_t t = seg;
-      for (int i = 0; i < 11; ++i) {
-        t *= 2u;
-        if (total(t) <= 0x7FFFFFFFull) break;
-      }
-      if (t > 1024u) { set_status(ctl, kESEG); return; }
-      seg = t;
-      adj = 1;
-    }
-  }
-  ctl->seg = seg;
-  ctl->adjusted = adj;
+  if (t > 1024u) return {kESEG, 0u, 0u};
+  return {kOK, t, 1u};
 }
 
 template <typename T>
@@ -109,7 +192,7 @@ __device__ __forceinline__ void fold_minmax(T v, typename TT<T>::U &mn_inv, type
 // A window that would run past N is skipped by the reference and its
 // min/max slot keeps the zero-filled scratch value, so it contributes 0.0.
 // Launch: 128 blocks x 256 threads, 8 windows per block.  The last block to
-// finish applies the host decision rules (seg_decide).
+// finish applies the host decision rules (decide_seg).
 template <typename T>
 __global__ void __launch_bounds__(256) seg_sample_kernel(const T *__restrict__ x, const T *__restrict__ y,
                                                          const T *__restrict__ z, uint64_t n, uint32_t dim,
@@ -161,8 +244,59 @@ __global__ void __launch_bounds__(256) seg_sample_kernel(const T *__restrict__ x
         mm[3 + d] = 0;
       }
     }
-    seg_decide(mm, dim, seg_in, rel_mode, rel_eb, eb, safe31, ctl);
+    const SegDecision sd = decide_seg<T>(mm, dim, seg_in, rel_mode, rel_eb, eb, safe31);
+    if (sd.status != kOK) set_status(ctl, sd.status);
+    else {
+      ctl->seg = sd.seg;
+      ctl->adjusted = sd.adjusted;
+    }
   }
+}
+
+// The sampling windows of computeSegSize restricted to one shard
+// [begin, begin + count) of a larger array (pointers start at `begin`): folds
+// the shard's share of every window into ctl->mm (windows past n contribute
+// 0.0, as in seg_sample_kernel).  Combining the shards' accumulators with an
+// unsigned max gives exactly the whole array's.
+template <typename T>
+__global__ void __launch_bounds__(256) seg_sample_shard_kernel(const T *__restrict__ x, const T *__restrict__ y,
+                                                               const T *__restrict__ z, uint64_t n, uint64_t begin,
+                                                               uint64_t count, uint32_t dim, Control *ctl) {
+  using U = typename TT<T>::U;
+  __shared__ U red[6][8];
+  const unsigned long long L = 256, B = 1024;
+  const unsigned long long stride = max((n - L) / B, 1ull);
+  U acc[6] = {0, 0, 0, 0, 0, 0};
+  const T *X[3] = {x, y, z};
+  for (int w = 0; w < 8; ++w) {
+    const unsigned long long win = (unsigned long long)blockIdx.x * 8 + w;
+    const unsigned long long st = win * stride;
+    if (st + L > n) {
+      for (uint32_t d = 0; d < dim; ++d) fold_minmax<T>((T)0, acc[2 * d], acc[2 * d + 1]);
+      continue;
+    }
+    const unsigned long long p = st + threadIdx.x;
+    if (p >= begin && p - begin < count)
+      for (uint32_t d = 0; d < dim; ++d) fold_minmax<T>(X[d][p - begin], acc[2 * d], acc[2 * d + 1]);
+  }
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int k = 0; k < 6; ++k) {
+    const U v = warp_max(acc[k]);
+    if (lane == 0) red[k][warp] = v;
+  }
+  __syncthreads();
+  if (threadIdx.x < 2 * dim) {
+    U v = 0;
+    for (int w = 0; w < 8; ++w) v = max(v, red[threadIdx.x][w]);
+    atomicMax(&ctl->mm[threadIdx.x], (unsigned long long)v);
+  }
+}
+
+// The segment size chosen by the caller is used as is (sharded compress).
+__global__ void set_seg_kernel(Control *ctl, uint32_t seg) {
+  ctl->seg = seg;
+  ctl->adjusted = 0;
 }
 
 // findMinimumValues<T> + convertRelEb<T> on the device.  The host scan starts

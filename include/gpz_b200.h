@@ -60,6 +60,12 @@ typedef struct gpz_params {
  * the reference format but differ from the reference's bytes when it fires. */
 #define GPZ_FLAG_SAFE31 1u
 
+/* Extension (not in the reference): use seg_size exactly as given -- no
+ * sampling, no automatic choice, no doubling.  Used by the sharded compress,
+ * where every shard must encode with the segment size decided once for the
+ * whole array (gpz_sample_minmax + gpz_decide_seg); seg_size must not be 0. */
+#define GPZ_FLAG_SEG_FIXED 2u
+
 /* Result of a compress / decompress call, read back from device scratch. */
 typedef struct gpz_result {
   uint64_t stream_bytes; /* compressed size (compress) */
@@ -185,6 +191,32 @@ int gpz_aos_to_soa(uint32_t float_bits, uint32_t dim, uint64_t n, const void *d_
                    void *d_y, void *d_z, void *stream);
 int gpz_soa_to_aos(uint32_t float_bits, uint32_t dim, uint64_t n, const void *d_x, const void *d_y,
                    const void *d_z, void *d_aos, void *stream);
+
+/* ---- sharded compress ------------------------------------------------------------
+ * One array compressed as shards on several GPUs (chunk-aligned ranges, each
+ * encoded as an ordinary stream with the common bound and segment size and
+ * stitched by offset).  No counterpart in the reference, which runs on one GPU;
+ * these split its computeSegSize (src/cudaWarpCompress.cu:1424-1557) and
+ * convertRelEb (src/main.cpp:35-55) into a per-shard part and a host part so
+ * the shards agree bit for bit with a single-GPU run.
+ *
+ * gpz_sample_minmax: the shard [begin, begin + count) of an n-point array
+ * (d_x.. point at element `begin`) folds its share of computeSegSize's sample
+ * windows into six ordered accumulators (x min, x max, y min, y max, z min,
+ * z max, as order-preserving unsigned keys with the minima complemented);
+ * combining the shards' accumulators with an unsigned max gives the whole
+ * array's.  Synchronises `stream`; needs gpz_decompress_scratch_bytes() of
+ * scratch.
+ * gpz_decide_seg: the segment-size rules on combined accumulators (host only).
+ * gpz_rel_abs_from_minmax: relative -> absolute bound from the combined
+ * per-axis minima and maxima of gpz_rel_to_abs (host only). */
+int gpz_sample_minmax(uint32_t float_bits, uint32_t dim, uint64_t n, uint64_t begin, uint64_t count,
+                      const void *d_x, const void *d_y, const void *d_z, void *d_scratch,
+                      uint64_t scratch_bytes, uint64_t *h_acc6, void *stream);
+int gpz_decide_seg(uint32_t float_bits, uint32_t dim, const uint64_t *acc6, uint32_t seg_in,
+                   int32_t rel_mode, double rel_eb, double eb, uint32_t flags, uint32_t *seg,
+                   uint32_t *adjusted);
+int gpz_rel_abs_from_minmax(uint32_t float_bits, const double *minmax6, double rel, double *eb);
 
 /* Total size in bytes of a compressed stream held on the device, from its
  * header, last offset-table entry and last meta record (three small copies;
