@@ -26,6 +26,7 @@ LIB_PATH = os.path.join(HERE, "libgpz_b200.so")
 GPZ_OK, GPZ_EINVAL, GPZ_ESEG, GPZ_ESTREAM, GPZ_ENOSPACE, GPZ_ECUDA, GPZ_ETIMEOUT, GPZ_ENOTSUP, GPZ_ELIMIT = range(9)
 GPZ_FLAG_SAFE31 = 1
 GPZ_FLAG_SEG_FIXED = 2
+GPZ_FLAG_REL_ON_DEVICE = 4
 ERRORS = {1: "EINVAL", 2: "ESEG", 3: "ESTREAM", 4: "ENOSPACE", 5: "ECUDA", 6: "ETIMEOUT", 7: "ENOTSUP", 8: "ELIMIT"}
 
 
@@ -49,6 +50,15 @@ class Result(ctypes.Structure):
 _VP = ctypes.c_void_p
 _U64 = ctypes.c_uint64
 _U32 = ctypes.c_uint32
+
+
+class BatchItem(ctypes.Structure):
+    """gpz_batch_item: one snapshot of a batched compress."""
+    _fields_ = [("float_bits", ctypes.c_uint32), ("dim", ctypes.c_uint32), ("n", ctypes.c_uint64),
+                ("d_x", ctypes.c_void_p), ("d_y", ctypes.c_void_p), ("d_z", ctypes.c_void_p),
+                ("d_out", ctypes.c_void_p), ("out_capacity", ctypes.c_uint64), ("eb", ctypes.c_double),
+                ("rel_eb", ctypes.c_double), ("rel_mode", ctypes.c_int32), ("seg_size", ctypes.c_uint32),
+                ("flags", ctypes.c_uint32), ("reserved", ctypes.c_uint32)]
 
 # name -> (restype, argtypes); the exported surface of include/gpz_b200.h
 SIGNATURES = {
@@ -80,6 +90,11 @@ SIGNATURES = {
                                       ctypes.c_double, _U32, ctypes.POINTER(_U32), ctypes.POINTER(_U32)]),
     "gpz_rel_abs_from_minmax": (ctypes.c_int, [_U32, ctypes.POINTER(ctypes.c_double), ctypes.c_double,
                                                ctypes.POINTER(ctypes.c_double)]),
+    "gpz_batch_create": (ctypes.c_int, [ctypes.POINTER(BatchItem), _U32, ctypes.POINTER(_VP), ctypes.POINTER(_U32)]),
+    "gpz_batch_launch": (ctypes.c_int, [_VP, _VP]),
+    "gpz_batch_results": (ctypes.c_int, [_VP, ctypes.POINTER(Result), ctypes.POINTER(ctypes.c_double), _VP]),
+    "gpz_batch_device_bytes": (_U64, [_VP]),
+    "gpz_batch_destroy": (ctypes.c_int, [_VP]),
 }
 
 _lib = None

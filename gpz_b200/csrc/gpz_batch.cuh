@@ -1,0 +1,159 @@
+// gpz_batch.cuh -- batched compress: many snapshots of one (float type,
+// dimension) class in one persistent launch.
+//
+// The reference compresses one snapshot per call (CompressorManager::compressWarp,
+// src/CompressorManager.cpp:12-16), so a workload of many small snapshots is
+// dominated by per-call launches, syncs and an almost idle GPU.  Here every
+// snapshot keeps its own stream, control block and look-back words; the
+// groups of 8 chunks of all snapshots of a class form one global work list
+// (snapshot after snapshot, so each snapshot's groups are claimed in order),
+// and one persistent kernel per class claims them.  A snapshot's stream is
+// byte-identical to the one gpz_compress writes for it: the per-chunk
+// encoder, the placement and the header/meta writes are the same code.
+#pragma once
+
+#include "gpz_kernels.cuh"
+#include "gpz_encode.cuh"
+
+namespace gpzb {
+
+constexpr uint32_t kBatchSegFixed = 1u;  // the segment size is given (no sampling)
+constexpr uint32_t kBatchSafe31 = 2u;    // GPZ_FLAG_SAFE31 rules for the automatic segment size
+constexpr uint32_t kBatchRelDev = 4u;    // absolute bound computed on the device from rel_eb
+constexpr int kBatchLocalBits = 40;      // map entry: item << 40 | group within the item
+
+// One snapshot of a batch.  `a` is what the single-stream kernel gets as its
+// parameter; a.eb is rewritten on the device when kBatchRelDev is set.
+template <typename T>
+struct BItem {
+  CArgs<T> a;
+  Control *rctl;     // control block of the device rel->abs reduction
+  T rel_eb;
+  uint32_t seg_in;
+  int32_t rel_mode;
+  uint32_t flags;
+};
+
+// computeSegSize for every snapshot of the class (blockIdx.y = snapshot, 128
+// blocks each), or the given segment size.
+template <typename T>
+__global__ void __launch_bounds__(256) batch_sample_kernel(const BItem<T> *items) {
+  const BItem<T> &it = items[blockIdx.y];
+  if (it.flags & kBatchSegFixed) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+      it.a.ctl->seg = it.seg_in;
+      it.a.ctl->adjusted = 0;
+    }
+    return;
+  }
+  seg_sample_block<T>(it.a.x, it.a.y, it.a.z, it.a.n, it.a.dim, it.seg_in, it.rel_mode, it.rel_eb, it.a.eb,
+                      (it.flags & kBatchSafe31) ? 1 : 0, it.a.ctl, blockIdx.x, gridDim.x);
+}
+
+struct BatchGroup {
+  uint32_t sz[kEncWarps];     // payload bytes of each warp's chunk
+  unsigned long long goff;    // stream offset of the group (~0: look-back gave up)
+  unsigned long long next;    // next global group
+  unsigned long long nmap;    // its map entry
+};
+
+// The compress loop of compress_kernel over a work list of many snapshots:
+// map[g] = snapshot << 40 | group of global group g.  The arguments of the
+// current and the next group's snapshot live in shared memory (double
+// buffered: the next group's points are loaded during the current group's
+// look-back and copy-out).  A snapshot whose segment size could not be
+// chosen (sampling error, status set) is skipped as a whole.
+template <typename T, int DIM>
+__global__ void __launch_bounds__(32 * kEncWarps, GPZ_ENC_MIN_CTAS)
+    compress_batch_kernel(const BItem<T> *__restrict__ items, const unsigned long long *__restrict__ map,
+                          unsigned long long total, unsigned long long *claim) {
+  using Tr = TT<T>;
+  constexpr bool is64 = sizeof(T) == 8;
+  constexpr uint32_t FULL = 0xFFFFFFFFu;
+  constexpr unsigned long long kLocal = (1ull << kBatchLocalBits) - 1;
+  extern __shared__ __align__(16) uint32_t enc_smem[];
+  __shared__ BatchGroup eg;
+  __shared__ CArgs<T> args[2];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  uint32_t *const sw = enc_smem + warp * kEncWords;
+  auto claim_next = [&](int slot) {  // thread 0
+    const unsigned long long g = atomicAdd(claim, 1ull);
+    eg.next = g;
+    // past the end: the first snapshot's first group stands in, so the
+    // prefetch below needs no condition (its loads are never used)
+    const unsigned long long m = g < total ? map[g] : 0ull;
+    eg.nmap = m;
+    args[slot] = items[m >> kBatchLocalBits].a;
+  };
+  if (threadIdx.x == 0) claim_next(0);
+  __syncthreads();
+  ChunkPoints<T, DIM> pts;
+  pts.load(args[0], (eg.nmap & kLocal) * kEncWarps + warp, lane);
+  int slot = 0;
+  for (;;) {
+    const unsigned long long g = eg.next;
+    if (g >= total) break;
+    const unsigned long long m = eg.nmap;
+    __syncthreads();  // B0: everyone has the group before it is replaced
+    if (threadIdx.x == 0) claim_next(slot ^ 1);
+    const CArgs<T> &a = args[slot];
+    Control *ctl = a.ctl;
+    const unsigned long long G = a.G;
+    const unsigned long long gid = m & kLocal, gbase = gid * kEncWarps;
+    const uint32_t seg = ctl->seg;  // 0: the snapshot's sampling failed
+    const bool live = seg != 0;
+    const uint32_t sh = live ? (uint32_t)__ffs((int)seg) - 1u : 0u, msk = seg - 1u;
+    const T eb = a.eb;
+    const T inv = is64 ? (T)__ddiv_rn(1.0, __dmul_rn(2.0, (double)eb)) : (T)__fdiv_rn(1.0f, __fmul_rn(2.0f, (float)eb));
+    const unsigned long long pay_base = Tr::hdr + 8ull * G + (unsigned long long)Tr::meta * G;
+    const unsigned long long c = gbase + warp;
+    uint32_t payload = 0, meta_word = 0;
+    if (live && c < G) payload = encode_chunk<T, DIM>(a, c, sw, seg, sh, msk, inv, pts, meta_word, lane);
+    if (lane == 0) eg.sz[warp] = payload;
+    __syncthreads();  // B1: the group's sizes are known (and the next group's snapshot)
+    pts.load(args[slot ^ 1], (eg.nmap & kLocal) * kEncWarps + warp, lane);  // in flight during the look-back and copy-out
+    if (live && warp == 0) {
+      const uint32_t s = lane < kEncWarps ? eg.sz[lane] : 0u;
+      const uint32_t tot = __reduce_add_sync(FULL, s);
+      if (lane == 0) publish_aggregate(a.look, gid, tot);
+      unsigned long long excl = 0;
+      const bool ok = resolve_prefix(a.look, gid, tot, ctl, excl);
+      if (lane == 0) eg.goff = ok ? excl : ~0ull;
+    }
+    __syncthreads();  // B2: the group's stream offset is known
+    const unsigned long long goff = eg.goff;
+    if (live && c < G && goff != ~0ull) {
+      unsigned long long off = goff;
+      for (int w = 0; w < warp; ++w) off += eg.sz[w];
+      if (lane == 0) reinterpret_cast<unsigned long long *>(a.out + Tr::hdr)[c] = off;
+      uint8_t *meta = a.out + Tr::hdr + 8ull * G + (unsigned long long)Tr::meta * c;
+      if (lane < (int)(Tr::meta / 4)) reinterpret_cast<uint32_t *>(meta)[lane] = meta_word;
+      if (c == 0) {
+        uint32_t *h = reinterpret_cast<uint32_t *>(a.out);
+        if (lane == 0) h[0] = a.dim;
+        if (lane == 1) h[1] = (uint32_t)a.n;
+        if (lane == 2) h[2] = (uint32_t)(a.n >> 32);
+        if (lane == 3) h[3] = Tr::bits;
+        if (!is64) {
+          if (lane == 4) h[4] = __float_as_uint((float)a.eb);
+          if (lane == 5) h[5] = seg;
+        } else {
+          if (lane == 4) h[4] = (uint32_t)__double_as_longlong((double)a.eb);
+          if (lane == 5) h[5] = (uint32_t)((unsigned long long)__double_as_longlong((double)a.eb) >> 32);
+          if (lane == 6) h[6] = seg;
+          if (lane == 7) h[7] = 32u;
+        }
+      }
+      if (pay_base + off + payload > a.out_cap) {
+        if (lane == 0) set_status(ctl, kENOSPACE);
+      } else {
+        uint32_t *dst = reinterpret_cast<uint32_t *>(a.out + pay_base + off);
+        for (uint32_t w = lane; w < payload / 4u; w += 32) dst[w] = sw[w];
+      }
+      if (c == G - 1 && lane == 0) ctl->stream_bytes = pay_base + off + payload;
+    }
+    slot ^= 1;
+  }
+}
+
+}  // namespace gpzb

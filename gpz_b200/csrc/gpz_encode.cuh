@@ -58,7 +58,7 @@ __device__ __forceinline__ uint32_t sx(uint32_t i) { return (uint32_t)swz((int)i
 // Ascending in-place bitonic sort of the n = hi - lo values a[sx(lo..hi)) by
 // one warp (variant whose exchanges all put the minimum at the lower index,
 // virtually padded with +inf up to a power of two).
-__device__ void warp_bitonic_u32(uint32_t *a, uint32_t lo, uint32_t n, int lane) {
+static __device__ void warp_bitonic_u32(uint32_t *a, uint32_t lo, uint32_t n, int lane) {
   uint32_t P = 2;
   while (P < n) P <<= 1;
   for (uint32_t k = 2; k <= P; k <<= 1) {
@@ -157,7 +157,7 @@ __device__ __forceinline__ void cas_up(uint32_t &x, uint32_t &y) {
 // distance >= 32 run on the transposed matrix (lane L holding elements
 // 32j + L), where distance-d pairs are registers j, j + d/32 and the mirrored
 // pairs are register j ^ (k/32 - 1) of lane 31 - L.
-__device__ __noinline__ void warp_sort1024_rows(uint32_t *rows, uint32_t *tsm, int lane) {
+static __device__ __noinline__ void warp_sort1024_rows(uint32_t *rows, uint32_t *tsm, int lane) {
   constexpr uint32_t FULL = 0xFFFFFFFFu;
   uint32_t v[32];
 #pragma unroll
@@ -258,7 +258,7 @@ __device__ __forceinline__ void put_planes(uint32_t *stage, uint32_t pos0, uint3
 // entry S's row l holds lane l's block ids; on exit S's row l holds the
 // sorted block ids of positions 32l..32l+31 and the first 16 words of hist's
 // row l the ranks r of positions j, j+16 as 16-bit pairs.
-__device__ __noinline__ void rank_wide(uint32_t *sw, uint32_t kmin, uint32_t cbits_all, uint32_t nvalid, int lane) {
+static __device__ __noinline__ void rank_wide(uint32_t *sw, uint32_t kmin, uint32_t cbits_all, uint32_t nvalid, int lane) {
   constexpr uint32_t FULL = 0xFFFFFFFFu;
   uint32_t *const S = sw, *const hist = sw + kChunk;
   const bool full = nvalid == (uint32_t)kChunk;

@@ -193,11 +193,13 @@ __device__ __forceinline__ void fold_minmax(T v, typename TT<T>::U &mn_inv, type
 // min/max slot keeps the zero-filled scratch value, so it contributes 0.0.
 // Launch: 128 blocks x 256 threads, 8 windows per block.  The last block to
 // finish applies the host decision rules (decide_seg).
+// One block's share (8 windows) of the sampling; `block` of `nblocks`
+// (128 blocks cover the 1024 windows).
 template <typename T>
-__global__ void __launch_bounds__(256) seg_sample_kernel(const T *__restrict__ x, const T *__restrict__ y,
-                                                         const T *__restrict__ z, uint64_t n, uint32_t dim,
-                                                         uint32_t seg_in, int rel_mode, T rel_eb, T eb,
-                                                         int safe31, Control *ctl) {
+__device__ __forceinline__ void seg_sample_block(const T *__restrict__ x, const T *__restrict__ y,
+                                                 const T *__restrict__ z, uint64_t n, uint32_t dim, uint32_t seg_in,
+                                                 int rel_mode, T rel_eb, T eb, int safe31, Control *ctl,
+                                                 unsigned block, unsigned nblocks) {
   using U = typename TT<T>::U;
   __shared__ U red[6][8];
   __shared__ int last;
@@ -206,7 +208,7 @@ __global__ void __launch_bounds__(256) seg_sample_kernel(const T *__restrict__ x
   U acc[6] = {0, 0, 0, 0, 0, 0};  // [min_inv, max] per axis
   const T *X[3] = {x, y, z};
   for (int w = 0; w < 8; ++w) {
-    const unsigned long long win = (unsigned long long)blockIdx.x * 8 + w;
+    const unsigned long long win = (unsigned long long)block * 8 + w;
     const unsigned long long st = win * stride;
     if (st + L > n) {
       for (uint32_t d = 0; d < dim; ++d) fold_minmax<T>((T)0, acc[2 * d], acc[2 * d + 1]);
@@ -228,7 +230,7 @@ __global__ void __launch_bounds__(256) seg_sample_kernel(const T *__restrict__ x
   }
   __threadfence();
   __syncthreads();
-  if (threadIdx.x == 0) last = (atomicAdd(&ctl->sample_done, 1u) == gridDim.x - 1);
+  if (threadIdx.x == 0) last = (atomicAdd(&ctl->sample_done, 1u) == nblocks - 1);
   __syncthreads();
   if (last && threadIdx.x == 0) {
     __threadfence();
@@ -251,6 +253,14 @@ __global__ void __launch_bounds__(256) seg_sample_kernel(const T *__restrict__ x
       ctl->adjusted = sd.adjusted;
     }
   }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) seg_sample_kernel(const T *__restrict__ x, const T *__restrict__ y,
+                                                         const T *__restrict__ z, uint64_t n, uint32_t dim,
+                                                         uint32_t seg_in, int rel_mode, T rel_eb, T eb,
+                                                         int safe31, Control *ctl) {
+  seg_sample_block<T>(x, y, z, n, dim, seg_in, rel_mode, rel_eb, eb, safe31, ctl, blockIdx.x, gridDim.x);
 }
 
 // The sampling windows of computeSegSize restricted to one shard
@@ -294,7 +304,7 @@ __global__ void __launch_bounds__(256) seg_sample_shard_kernel(const T *__restri
 }
 
 // The segment size chosen by the caller is used as is (sharded compress).
-__global__ void set_seg_kernel(Control *ctl, uint32_t seg) {
+static __global__ void set_seg_kernel(Control *ctl, uint32_t seg) {
   ctl->seg = seg;
   ctl->adjusted = 0;
 }
@@ -302,10 +312,13 @@ __global__ void set_seg_kernel(Control *ctl, uint32_t seg) {
 // findMinimumValues<T> + convertRelEb<T> on the device.  The host scan starts
 // from float limits (include/utils.cuh:48-53) and ignores NaNs; 2D data has
 // z == 0 (utils.cuh:141).
+// One block (`block` of `nblocks`) of the grid-stride min/max; the last block
+// to finish converts, stores the bound in ctl->out_eb and, when eb_out is
+// given, in *eb_out.
 template <typename T>
-__global__ void __launch_bounds__(256) rel_to_abs_kernel(const T *__restrict__ x, const T *__restrict__ y,
-                                                         const T *__restrict__ z, uint64_t n, uint32_t dim,
-                                                         T rel, Control *ctl) {
+__device__ __forceinline__ void rel_to_abs_block(const T *__restrict__ x, const T *__restrict__ y,
+                                                 const T *__restrict__ z, uint64_t n, uint32_t dim, T rel,
+                                                 Control *ctl, T *eb_out, unsigned block, unsigned nblocks) {
   using U = typename TT<T>::U;
   __shared__ U red[6][8];
   __shared__ int last;
@@ -316,8 +329,8 @@ __global__ void __launch_bounds__(256) rel_to_abs_kernel(const T *__restrict__ x
     acc[2 * d + 1] = ord_of((T)(-FLT_MAX));
   }
   const T *X[3] = {x, y, z};
-  const unsigned long long step = (unsigned long long)gridDim.x * blockDim.x;
-  for (unsigned long long i = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += step)
+  const unsigned long long step = (unsigned long long)nblocks * blockDim.x;
+  for (unsigned long long i = (unsigned long long)block * blockDim.x + threadIdx.x; i < n; i += step)
     for (uint32_t d = 0; d < dim; ++d) fold_minmax<T>(X[d][i], acc[2 * d], acc[2 * d + 1]);
   if (dim == 2) fold_minmax<T>((T)0, acc[4], acc[5]);
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -334,7 +347,7 @@ __global__ void __launch_bounds__(256) rel_to_abs_kernel(const T *__restrict__ x
   }
   __threadfence();
   __syncthreads();
-  if (threadIdx.x == 0) last = (atomicAdd(&ctl->sample_done, 1u) == gridDim.x - 1);
+  if (threadIdx.x == 0) last = (atomicAdd(&ctl->sample_done, 1u) == nblocks - 1);
   __syncthreads();
   if (last && threadIdx.x == 0) {
     __threadfence();
@@ -356,7 +369,15 @@ __global__ void __launch_bounds__(256) rel_to_abs_kernel(const T *__restrict__ x
       r = (T)__dmul_rn(fmax(fmax(xr, yr), zr), (double)rel);
     }
     ctl->out_eb = (double)r;
+    if (eb_out) *eb_out = r;
   }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) rel_to_abs_kernel(const T *__restrict__ x, const T *__restrict__ y,
+                                                         const T *__restrict__ z, uint64_t n, uint32_t dim,
+                                                         T rel, Control *ctl) {
+  rel_to_abs_block<T>(x, y, z, n, dim, rel, ctl, nullptr, blockIdx.x, gridDim.x);
 }
 
 // ===========================================================================
@@ -389,7 +410,7 @@ __device__ __forceinline__ void publish_aggregate(unsigned long long *look, unsi
 
 // Warp-collective.  Returns false when a bounded wait gave up or another CTA
 // aborted (the kernel then stops taking chunks and reports GPZ_ETIMEOUT).
-__device__ bool resolve_prefix(unsigned long long *look, unsigned long long c, unsigned long long agg,
+static __device__ bool resolve_prefix(unsigned long long *look, unsigned long long c, unsigned long long agg,
                                Control *ctl, unsigned long long &excl_out) {
   const int lane = threadIdx.x & 31;
   if (c == 0) {

@@ -227,6 +227,56 @@ int gpz_rel_abs_from_minmax(uint32_t float_bits, const double *minmax6, double r
  * stream it validates. */
 int gpz_stream_size(const void *d_stream, uint64_t cap, uint64_t *bytes, void *stream);
 
+/* ---- batched compress -------------------------------------------------------------
+ * No counterpart in the reference, which compresses one snapshot per call
+ * (CompressorManager::compressWarp, src/CompressorManager.cpp:12-16; each call
+ * samples, launches and synchronises on its own).  A batch compresses many
+ * snapshots of mixed size, float width and dimension with one CUDA graph:
+ * device rel->abs bounds, segment-size sampling and one persistent compress
+ * kernel per (float width, dimension) class whose work list holds the 8-chunk
+ * groups of all its snapshots.  Every snapshot's stream is byte-identical to
+ * what gpz_compress writes for the same parameters.
+ *
+ * A batch is a plan bound to the buffers named in its items (like an FFT
+ * plan): gpz_batch_create validates the items, allocates the batch's device
+ * memory (descriptors, work maps, one control block and look-back words per
+ * snapshot) and captures the graph; gpz_batch_launch replays it on a stream
+ * (the inputs may change between launches, the pointers and sizes may not);
+ * gpz_batch_results synchronises the stream and reads every snapshot's result.
+ * Launches of one batch must not overlap on the GPU. */
+typedef struct gpz_batch_item {
+  uint32_t float_bits;   /* 32 or 64 */
+  uint32_t dim;          /* 2 or 3 */
+  uint64_t n;            /* points, >= 1 */
+  const void *d_x;       /* SoA device arrays; d_z is ignored for dim == 2 */
+  const void *d_y;
+  const void *d_z;
+  void *d_out;           /* the snapshot's stream */
+  uint64_t out_capacity; /* bytes at d_out */
+  double eb;             /* absolute bound (ignored with GPZ_FLAG_REL_ON_DEVICE) */
+  double rel_eb;         /* relative bound: segment-size rules; with GPZ_FLAG_REL_ON_DEVICE also the bound */
+  int32_t rel_mode;      /* 1: the "rel" error mode of the segment-size rules */
+  uint32_t seg_size;     /* 0: automatic; see GPZ_FLAG_SEG_FIXED */
+  uint32_t flags;        /* GPZ_FLAG_SAFE31 | GPZ_FLAG_SEG_FIXED | GPZ_FLAG_REL_ON_DEVICE */
+  uint32_t reserved;     /* 0 */
+} gpz_batch_item;
+
+/* Batch item flag: the absolute bound is computed on the device from rel_eb
+ * exactly as gpz_rel_to_abs computes it. */
+#define GPZ_FLAG_REL_ON_DEVICE 4u
+
+typedef struct gpz_batch gpz_batch;
+
+/* GPZ_EINVAL names no item; *bad_item (may be NULL) receives the index of the
+ * first invalid item. */
+int gpz_batch_create(const gpz_batch_item *items, uint32_t count, gpz_batch **batch, uint32_t *bad_item);
+int gpz_batch_launch(gpz_batch *batch, void *stream);
+/* results[count]; h_eb (may be NULL) receives each snapshot's absolute bound. */
+int gpz_batch_results(gpz_batch *batch, gpz_result *results, double *h_eb, void *stream);
+/* Device memory the batch holds (bytes). */
+uint64_t gpz_batch_device_bytes(const gpz_batch *batch);
+int gpz_batch_destroy(gpz_batch *batch);
+
 /* Library version string. */
 const char *gpz_version(void);
 
