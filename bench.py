@@ -368,6 +368,179 @@ def run_ours(args):
         dist.destroy_process_group()
 
 
+BATCH_WORKLOAD = ("256 independent snapshots, sizes log-uniform in [1e4, 2e7] points, 75% 3D / 25% 2D, "
+                  "85% float32 / 15% float64, each uniform i.i.d. in [0, L)^dim with L = 100 * (n / 1e6)^(1/dim) "
+                  "(the 1M-point [0,100)^3 generator at the same density), rel error bound drawn from "
+                  "{1e-3, 1e-4, 1e-5}, automatic segment size")
+
+
+def batch_specs(count, seed):
+    import math
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(count):
+        n = int(round(math.exp(rng.uniform(math.log(1e4), math.log(2e7)))))
+        dim = 3 if rng.random() < 0.75 else 2
+        bits = 32 if rng.random() < 0.85 else 64
+        rel = (1e-3, 1e-4, 1e-5)[int(rng.integers(3))]
+        out.append((n, dim, bits, rel))
+    return out
+
+
+def run_batched(args):
+    """Batched form: all snapshots compressed by one graph launch (device
+    rel->abs, sampling, per-class persistent kernels) and decoded by one,
+    against the same snapshots through per-snapshot calls.  Prints one JSON
+    line; the stream bytes and reconstructions of both forms are compared."""
+    import numpy as np
+    import torch
+    import gpz_b200 as gz
+    from gpz_b200.batch import Batch, DecompressBatch, Snapshot, autotune
+    dev = torch.device("cuda", 0)
+    specs = batch_specs(args.batch, 4321)
+    snaps = []
+    g = torch.Generator(device=dev)
+    for i, (n, dim, bits, rel) in enumerate(specs):
+        g.manual_seed(1000 + i)
+        L = 100.0 * (n / 1e6) ** (1.0 / dim)
+        dt = torch.float32 if bits == 32 else torch.float64
+        xyz = [torch.rand(n, generator=g, device=dev, dtype=dt) * L for _ in range(dim)]
+        snaps.append((xyz[0], xyz[1], xyz[2] if dim == 3 else None, rel))
+    inb = sum(n * dim * bits // 8 for n, dim, bits, _ in specs)
+    stream = torch.cuda.current_stream(dev)
+
+    def ev_time(fn, reps):
+        for _ in range(max(args.warmup, 3)):
+            fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(reps):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps
+
+    # ---- batched
+    b = Batch([Snapshot(x, y, z, rel_eb=rel) for x, y, z, rel in snaps])
+    t_bc = ev_time(lambda: b.launch(stream), args.steps)
+    res = b.results()
+    assert all(r.status == 0 for r, _ in res), [r.status for r, _ in res]
+    streams = b.streams()
+    d = DecompressBatch(streams)
+    t_bd = ev_time(lambda: d.launch(stream), args.steps)
+    assert all(st == 0 for st in d.results())
+    cbytes = sum(int(r.stream_bytes) for r, _ in res)
+
+    # ---- per-snapshot calls: rel->abs on the device (a synchronising call
+    # that returns the bound to the host) then compress, as a user of the
+    # single-stream API does; and compress alone with the bounds known
+    ebs = [eb for _, eb in res]
+    plain_out = [torch.empty(gz.stream_bound(x.numel(), 3 if z is not None else 2, 32 if x.dtype == torch.float32 else 64),
+                             dtype=torch.uint8, device=dev) for x, y, z, _ in snaps]
+    plain_scr = [torch.empty(gz.compress_scratch_bytes(x.numel()), dtype=torch.uint8, device=dev) for x, _, _, _ in snaps]
+    params = []
+    for (x, y, z, rel), eb in zip(snaps, ebs):
+        bits = 32 if x.dtype == torch.float32 else 64
+        params.append(gz.make_params(x.numel(), 3 if z is not None else 2, bits, eb, 0, True,
+                                     float(np.float32(rel)) if bits == 32 else rel))
+
+    def plain_with_rel():
+        for (x, y, z, rel), p, o, sc in zip(snaps, params, plain_out, plain_scr):
+            gz.rel_to_abs(x, y, z, rel, stream)
+            gz.compress_into(p, x, y, z if z is not None else x, o, sc, stream, sync=False)
+
+    def plain_compress():
+        for (x, y, z, _), p, o, sc in zip(snaps, params, plain_out, plain_scr):
+            gz.compress_into(p, x, y, z if z is not None else x, o, sc, stream, sync=False)
+
+    # the batch with the bounds given (no device rel->abs), the counterpart of
+    # the compress-only per-snapshot arm
+    b2 = Batch([Snapshot(x, y, z, eb=eb, rel_eb=rel, rel_mode=True) for (x, y, z, rel), eb in zip(snaps, ebs)])
+    t_bc2 = ev_time(lambda: b2.launch(stream), args.steps)
+    res2 = b2.results()
+    same = all(r.status == 0 for r, _ in res2) and all(
+        torch.equal(o, s_b) for o, s_b in zip(b2.streams(), streams))
+    b2.close()
+    t_pcr = ev_time(plain_with_rel, max(1, args.steps // 2))
+    t_pc = ev_time(plain_compress, args.steps)
+    for (x, _, _, _), o, sc, s_b in zip(snaps, plain_out, plain_scr, streams):
+        r = gz.result_get(sc, stream)
+        same &= r.status == 0 and r.stream_bytes == s_b.numel() and torch.equal(o[: r.stream_bytes], s_b)
+    dec_out = [tuple(torch.empty_like(x) if t is not None else None for t in (x, y, z)) for x, y, z, _ in snaps]
+    dscr = [torch.empty(256, dtype=torch.uint8, device=dev) for _ in snaps]
+
+    def plain_decompress():
+        for s_b, (ox, oy, oz), (x, _, z, _), sc in zip(streams, dec_out, snaps, dscr):
+            dim = 3 if z is not None else 2
+            gz.decompress_into(s_b, s_b.numel(), 32 if x.dtype == torch.float32 else 64, dim, ox, oy,
+                               oz if dim == 3 else ox, sc, stream, sync=False)
+
+    t_pd = ev_time(plain_decompress, args.steps)
+    torch.cuda.synchronize()
+    for (ox, oy, oz), (bx, by, bz) in zip(dec_out, d.outputs):
+        for a, c in ((ox, bx), (oy, by), (oz, bz)):
+            if a is not None:
+                same &= torch.equal(a.view(torch.uint8), c.view(torch.uint8))
+    # ---- autotuned segment sizes: the batch and the per-snapshot calls with
+    # the same (fixed) segment sizes
+    tsnaps = [Snapshot(x, y, z, rel_eb=rel) for x, y, z, rel in snaps]
+    tt0 = time.perf_counter()
+    recs = autotune(tsnaps, stream=stream)
+    tune_s = time.perf_counter() - tt0
+    bt = Batch(tsnaps)
+    t_bt = ev_time(lambda: bt.launch(stream), args.steps)
+    rt = bt.results()
+    tuned_streams = bt.streams()
+    tuned_bytes = sum(int(r.stream_bytes) for r, _ in rt)
+    tparams = []
+    for (x, y, z, rel), snap, eb in zip(snaps, tsnaps, ebs):
+        bits = 32 if x.dtype == torch.float32 else 64
+        p = gz.make_params(x.numel(), 3 if z is not None else 2, bits, eb, snap.seg_size, True,
+                           float(np.float32(rel)) if bits == 32 else rel)
+        p.flags |= gz.GPZ_FLAG_SEG_FIXED
+        tparams.append(p)
+
+    def plain_tuned():
+        for (x, y, z, rel), p, o, sc in zip(snaps, tparams, plain_out, plain_scr):
+            gz.rel_to_abs(x, y, z, rel, stream)
+            gz.compress_into(p, x, y, z if z is not None else x, o, sc, stream, sync=False)
+
+    t_ptr = ev_time(plain_tuned, max(1, args.steps // 2))
+    for o, sc, s_b in zip(plain_out, plain_scr, tuned_streams):
+        r = gz.result_get(sc, stream)
+        same &= r.status == 0 and r.stream_bytes == s_b.numel() and torch.equal(o[: r.stream_bytes], s_b)
+    segs_default = [int(r.seg_size) for r, _ in res]
+    segs_tuned = [s.seg_size for s in tsnaps]
+    bt.close()
+    gbs = lambda ms: round(inb / (ms * 1e-3) / 1e9, 2)
+    line = {
+        "metric": "batched compress / decompress aggregate GB/s (input bytes) vs per-snapshot calls, 1 B200",
+        "unit": "GB/s", "n_gpus": 1, "steps": args.steps, "warmup": max(args.warmup, 3), "higher_is_better": True,
+        "data": "synthetic", "config": {"workload": BATCH_WORKLOAD, "snapshots": len(specs), "points": sum(s[0] for s in specs),
+                                        "input_bytes": inb, "stream_bytes": cbytes},
+        "batched": {"rel_and_compress_ms": round(t_bc, 3), "rel_and_compress_gbs": gbs(t_bc),
+                    "compress_ms": round(t_bc2, 3), "compress_gbs": gbs(t_bc2), "decompress_ms": round(t_bd, 3),
+                    "decompress_gbs": gbs(t_bd), "device_bytes": b.device_bytes},
+        "plain": {"rel_and_compress_ms": round(t_pcr, 3), "rel_and_compress_gbs": gbs(t_pcr),
+                  "compress_ms": round(t_pc, 3), "compress_gbs": gbs(t_pc),
+                  "decompress_ms": round(t_pd, 3), "decompress_gbs": gbs(t_pd)},
+        "speedup": {"rel_and_compress": round(t_pcr / t_bc, 3), "compress": round(t_pc / t_bc2, 3),
+                    "decompress": round(t_pd / t_bd, 3)},
+        "autotuned": {"rel_and_compress_ms": round(t_bt, 3), "rel_and_compress_gbs": gbs(t_bt),
+                      "plain_rel_and_compress_ms": round(t_ptr, 3), "speedup": round(t_ptr / t_bt, 3),
+                      "stream_bytes": tuned_bytes, "stream_bytes_default_seg": cbytes,
+                      "ratio_gain": round(cbytes / tuned_bytes, 4), "tune_seconds": round(tune_s, 3),
+                      "segments_changed": sum(a != b for a, b in zip(segs_default, segs_tuned)),
+                      "candidates": [1, 2, 4, 8, 16, 32, 64, 128], "sample_points": 1 << 17},
+        "identical_output": bool(same),
+    }
+    b.close()
+    d.close()
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -376,11 +549,16 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer end-to-end timing")
+    ap.add_argument("--batched", action="store_true",
+                    help="time the batched form (many snapshots per graph launch) against per-snapshot calls")
+    ap.add_argument("--batch", type=int, default=256, help="snapshots in the batched workload")
     ap.add_argument("--points", type=int, default=N_POINTS,
                     help="points per GPU (smaller cases for profiler captures; the headline uses the default)")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)
+    elif args.batched:
+        run_batched(args)
     else:
         run_ours(args)
 

@@ -60,6 +60,13 @@ class BatchItem(ctypes.Structure):
                 ("rel_eb", ctypes.c_double), ("rel_mode", ctypes.c_int32), ("seg_size", ctypes.c_uint32),
                 ("flags", ctypes.c_uint32), ("reserved", ctypes.c_uint32)]
 
+
+class DBatchItem(ctypes.Structure):
+    """gpz_dbatch_item: one stream of a batched decompress."""
+    _fields_ = [("d_stream", ctypes.c_void_p), ("stream_bytes", ctypes.c_uint64), ("float_bits", ctypes.c_uint32),
+                ("dim", ctypes.c_uint32), ("n", ctypes.c_uint64), ("d_x", ctypes.c_void_p), ("d_y", ctypes.c_void_p),
+                ("d_z", ctypes.c_void_p), ("out_capacity", ctypes.c_uint64)]
+
 # name -> (restype, argtypes); the exported surface of include/gpz_b200.h
 SIGNATURES = {
     "gpz_stream_bound": (_U64, [_U64, _U32, _U32]),
@@ -95,6 +102,11 @@ SIGNATURES = {
     "gpz_batch_results": (ctypes.c_int, [_VP, ctypes.POINTER(Result), ctypes.POINTER(ctypes.c_double), _VP]),
     "gpz_batch_device_bytes": (_U64, [_VP]),
     "gpz_batch_destroy": (ctypes.c_int, [_VP]),
+    "gpz_dbatch_create": (ctypes.c_int, [ctypes.POINTER(DBatchItem), _U32, ctypes.POINTER(_VP),
+                                         ctypes.POINTER(_U32)]),
+    "gpz_dbatch_launch": (ctypes.c_int, [_VP, _VP]),
+    "gpz_dbatch_results": (ctypes.c_int, [_VP, ctypes.POINTER(Result), _VP]),
+    "gpz_dbatch_destroy": (ctypes.c_int, [_VP]),
 }
 
 _lib = None

@@ -14,6 +14,7 @@
 
 #include "gpz_kernels.cuh"
 #include "gpz_encode.cuh"
+#include "gpz_decode.cuh"
 
 namespace gpzb {
 
@@ -153,6 +154,83 @@ __global__ void __launch_bounds__(32 * kEncWarps, GPZ_ENC_MIN_CTAS)
       if (c == G - 1 && lane == 0) ctl->stream_bytes = pay_base + off + payload;
     }
     slot ^= 1;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Batched decompress.
+// ---------------------------------------------------------------------------
+
+// One stream of a decompress batch; n is the point count the caller read
+// from the stream's header (the work map is built from it); G, pay_base, eb,
+// seg and ok come from the device-side header check.
+template <typename T>
+struct DItem {
+  DArgs<T> a;
+  unsigned long long n, G, pay_base;
+  T eb;
+  uint32_t seg;
+  int32_t ok;
+};
+
+// The header checks of decompress_kernel, once per stream (one thread each).
+template <typename T, int DIM>
+__global__ void dbatch_header_kernel(DItem<T> *items, uint32_t K) {
+  using Tr = TT<T>;
+  const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= K) return;
+  DItem<T> &it = items[k];
+  it.ok = 0;
+  Control *ctl = it.a.ctl;
+  if (it.a.bytes < Tr::hdr) { set_status(ctl, kESTREAM); return; }
+  const uint8_t *s = it.a.s;
+  const uint32_t dim = *reinterpret_cast<const uint32_t *>(s);
+  unsigned long long n;
+  memcpy(&n, s + 4, 8);
+  const uint32_t bits = *reinterpret_cast<const uint32_t *>(s + 12);
+  T eb;
+  memcpy(&eb, s + 16, sizeof(T));
+  const uint32_t seg = *reinterpret_cast<const uint32_t *>(s + 16 + sizeof(T));
+  const unsigned long long G = (n + kChunk - 1) / kChunk;
+  if (bits != Tr::bits || dim != (uint32_t)DIM || n == 0 || n != it.n || seg == 0 ||
+      G > (it.a.bytes - Tr::hdr) / (8ull + Tr::meta)) {
+    set_status(ctl, kESTREAM);
+    return;
+  }
+  if (n > it.a.cap) { set_status(ctl, kENOSPACE); return; }
+  it.G = G;
+  it.pay_base = Tr::hdr + 8ull * G + (unsigned long long)Tr::meta * G;
+  it.eb = eb;
+  it.seg = seg;
+  it.ok = 1;
+}
+
+// decompress_kernel over the chunks of many streams: warps stride over the
+// global chunk list, cmap[c] = stream << 40 | chunk within the stream.
+template <typename T, int DIM>
+__global__ void __launch_bounds__(32 * DecCfg<T>::warps, DecCfg<T>::min_ctas)
+    decompress_batch_kernel(const DItem<T> *__restrict__ items, const unsigned long long *__restrict__ cmap,
+                            unsigned long long total) {
+  using Cfg = DecCfg<T>;
+  constexpr int W = Cfg::warps;
+  constexpr unsigned long long kLocal = (1ull << kBatchLocalBits) - 1;
+  extern __shared__ __align__(16) uint32_t dec_smem[];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  uint32_t *const sw = dec_smem + warp * Cfg::words;
+  const unsigned long long nwarps = (unsigned long long)gridDim.x * W;
+  for (unsigned long long gc = (unsigned long long)blockIdx.x * W + warp; gc < total; gc += nwarps) {
+    const unsigned long long m = cmap[gc];
+    const DItem<T> &it = items[m >> kBatchLocalBits];
+    if (!it.ok) continue;
+    const DArgs<T> a = it.a;
+    const unsigned long long c = m & kLocal, G = it.G;
+    const uint32_t seg = it.seg;
+    ChunkGeom g;
+    g.seg = seg;
+    g.sh = (uint32_t)__ffs((int)seg) - 1u;
+    g.msk = seg - 1u;
+    const uint32_t mwc = dec_meta_word<T>(a.s, G, c, lane);
+    decode_chunk<T, DIM>(a, c, it.n, G, it.pay_base, it.eb, seg, g, mwc, sw, lane);
   }
 }
 

@@ -6,9 +6,9 @@
 //   [look-back words: one per 8-chunk group of every snapshot][claim counters]
 //     -- zeroed at the start of every launch (a memset node of the graph)
 //   [per class: item descriptors (BItem<T>), group map, rel-block map]
-// Classes are (float, 2D), (float, 3D), (double, 2D), (double, 3D); each runs
-// on its own branch of the graph: rel->abs (when any of its snapshots asks
-// for it), sampling, persistent compress.
+// Classes are (float, 2D), (float, 3D), (double, 2D), (double, 3D); the graph
+// runs them one after another: rel->abs (when any of its snapshots asks for
+// it), sampling, persistent compress.
 
 #include <algorithm>
 #include <cstring>
@@ -213,41 +213,30 @@ int gpz_batch_create(const gpz_batch_item *items, uint32_t count, gpz_batch **ba
   }
 
   // ---- graph: memset, then one branch per class
-  cudaStream_t s0 = nullptr, sc[4] = {nullptr, nullptr, nullptr, nullptr};
-  cudaEvent_t e0 = nullptr, ec[4] = {nullptr, nullptr, nullptr, nullptr};
+  cudaStream_t s0 = nullptr;
   cudaGraph_t graph = nullptr;
-  bool okc = cudaStreamCreateWithFlags(&s0, cudaStreamNonBlocking) == cudaSuccess &&
-             cudaEventCreateWithFlags(&e0, cudaEventDisableTiming) == cudaSuccess;
-  for (int c = 0; c < 4 && okc; ++c)
-    okc = cudaStreamCreateWithFlags(&sc[c], cudaStreamNonBlocking) == cudaSuccess &&
-          cudaEventCreateWithFlags(&ec[c], cudaEventDisableTiming) == cudaSuccess;
+  bool okc = cudaStreamCreateWithFlags(&s0, cudaStreamNonBlocking) == cudaSuccess;
   if (okc) okc = cudaStreamBeginCapture(s0, cudaStreamCaptureModeThreadLocal) == cudaSuccess;
   if (okc) {
+    // The classes run one after another: two different compress kernels
+    // resident on one SM thrash its instruction cache (each is a few hundred
+    // KB of unrolled code), which costs far more than the overlap gains.
     cudaMemsetAsync(b->mem, 0, b->zero_bytes, s0);
-    cudaEventRecord(e0, s0);
     for (int c = 0; c < 4; ++c) {
       if (cls[c].items.empty()) continue;
-      cudaStreamWaitEvent(sc[c], e0, 0);
       const uint64_t claim = claim_off + 8ull * c;
       switch (c) {
-        case 0: enqueue_class<float, 2>(cls[c], b->mem, claim, sc[c]); break;
-        case 1: enqueue_class<float, 3>(cls[c], b->mem, claim, sc[c]); break;
-        case 2: enqueue_class<double, 2>(cls[c], b->mem, claim, sc[c]); break;
-        default: enqueue_class<double, 3>(cls[c], b->mem, claim, sc[c]); break;
+        case 0: enqueue_class<float, 2>(cls[c], b->mem, claim, s0); break;
+        case 1: enqueue_class<float, 3>(cls[c], b->mem, claim, s0); break;
+        case 2: enqueue_class<double, 2>(cls[c], b->mem, claim, s0); break;
+        default: enqueue_class<double, 3>(cls[c], b->mem, claim, s0); break;
       }
-      cudaEventRecord(ec[c], sc[c]);
-      cudaStreamWaitEvent(s0, ec[c], 0);
     }
     okc = cudaStreamEndCapture(s0, &graph) == cudaSuccess && graph;
   }
   if (okc) okc = cudaGraphInstantiate(&b->exec, graph, 0) == cudaSuccess;
   if (graph) cudaGraphDestroy(graph);
-  for (int c = 0; c < 4; ++c) {
-    if (sc[c]) cudaStreamDestroy(sc[c]);
-    if (ec[c]) cudaEventDestroy(ec[c]);
-  }
   if (s0) cudaStreamDestroy(s0);
-  if (e0) cudaEventDestroy(e0);
   if (!okc) {
     cudaGetLastError();
     cudaFree(b->mem);
@@ -292,6 +281,193 @@ int gpz_batch_results(gpz_batch *b, gpz_result *results, double *h_eb, void *str
 uint64_t gpz_batch_device_bytes(const gpz_batch *b) { return b ? b->bytes : 0; }
 
 int gpz_batch_destroy(gpz_batch *b) {
+  if (!b) return GPZ_EINVAL;
+  if (b->exec) cudaGraphExecDestroy(b->exec);
+  if (b->mem) cudaFree(b->mem);
+  delete b;
+  return GPZ_OK;
+}
+
+}  // extern "C"
+
+// ===========================================================================
+// Batched decompress.
+// ===========================================================================
+namespace {
+
+template <typename T, int DIM>
+int dec_grid(uint64_t chunks) {
+  auto k = decompress_batch_kernel<T, DIM>;
+  constexpr size_t smem = dec_smem_bytes<T>();
+  constexpr int W = DecCfg<T>::warps;
+  if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) return -1;
+  int occ = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k, 32 * W, smem) != cudaSuccess || occ < 1) occ = 1;
+  return (int)std::min<uint64_t>((chunks + W - 1) / W, (uint64_t)num_sms_now() * occ);
+}
+
+struct DClass {
+  std::vector<uint32_t> items;
+  uint64_t chunks = 0, table_off = 0, map_off = 0;
+  int grid = 0;
+};
+
+template <typename T, int DIM>
+void enqueue_dclass(const DClass &cp, uint8_t *dev, cudaStream_t st) {
+  DItem<T> *tab = reinterpret_cast<DItem<T> *>(dev + cp.table_off);
+  const uint32_t K = (uint32_t)cp.items.size();
+  dbatch_header_kernel<T, DIM><<<(K + 127) / 128, 128, 0, st>>>(tab, K);
+  decompress_batch_kernel<T, DIM><<<cp.grid, 32 * DecCfg<T>::warps, dec_smem_bytes<T>(), st>>>(
+      tab, reinterpret_cast<const unsigned long long *>(dev + cp.map_off), cp.chunks);
+}
+
+template <typename T>
+void fill_ditem(DItem<T> &d, const gpz_dbatch_item &it, Control *ctl) {
+  memset(&d, 0, sizeof(d));
+  d.a.s = static_cast<const uint8_t *>(it.d_stream);
+  d.a.bytes = it.stream_bytes;
+  d.a.x = static_cast<T *>(it.d_x);
+  d.a.y = static_cast<T *>(it.d_y);
+  d.a.z = static_cast<T *>(it.dim == 3 ? it.d_z : it.d_y);
+  d.a.cap = it.out_capacity;
+  d.a.ctl = ctl;
+  auto al = [](const void *p) { return ((uintptr_t)p & 15u) == 0; };
+  d.a.vec_ok = al(it.d_x) && al(it.d_y) && (it.dim == 2 || al(it.d_z));
+  d.n = it.n;
+}
+
+}  // namespace
+
+struct gpz_dbatch {
+  uint32_t count = 0;
+  uint8_t *mem = nullptr;
+  uint64_t bytes = 0, zero_bytes = 0;
+  cudaGraphExec_t exec = nullptr;
+};
+
+extern "C" {
+
+int gpz_dbatch_create(const gpz_dbatch_item *items, uint32_t count, gpz_dbatch **batch, uint32_t *bad_item) {
+  if (!batch || !items || count == 0) return GPZ_EINVAL;
+  *batch = nullptr;
+  for (uint32_t i = 0; i < count; ++i) {
+    const gpz_dbatch_item &it = items[i];
+    const bool ok = (it.float_bits == 32 || it.float_bits == 64) && (it.dim == 2 || it.dim == 3) && it.n >= 1 &&
+                    it.d_stream && ((uintptr_t)it.d_stream & 7u) == 0 && it.d_x && it.d_y &&
+                    (it.dim == 2 || it.d_z) && it.out_capacity >= it.n;
+    if (!ok) {
+      if (bad_item) *bad_item = i;
+      return GPZ_EINVAL;
+    }
+  }
+  gpz_dbatch *b = new (std::nothrow) gpz_dbatch;
+  if (!b) return GPZ_ECUDA;
+  b->count = count;
+  DClass cls[4];
+  for (uint32_t i = 0; i < count; ++i) {
+    DClass &cp = cls[class_of(items[i].float_bits, items[i].dim)];
+    cp.items.push_back(i);
+    cp.chunks += (items[i].n + kChunk - 1) / kChunk;
+  }
+  b->zero_bytes = (uint64_t)count * kCtlBytes;
+  uint64_t off = align256(b->zero_bytes);
+  for (int c = 0; c < 4; ++c) {
+    if (cls[c].items.empty()) continue;
+    const uint64_t isz = c < 2 ? sizeof(DItem<float>) : sizeof(DItem<double>);
+    cls[c].table_off = off;
+    off = align256(off + isz * cls[c].items.size());
+    cls[c].map_off = off;
+    off = align256(off + 8 * cls[c].chunks);
+  }
+  b->bytes = off;
+  if (cudaMalloc(&b->mem, b->bytes) != cudaSuccess) {
+    delete b;
+    return GPZ_ECUDA;
+  }
+  std::vector<uint8_t> host(b->bytes - b->zero_bytes);
+  auto H = [&](uint64_t dev_off) { return host.data() + (dev_off - b->zero_bytes); };
+  for (int c = 0; c < 4; ++c) {
+    DClass &cp = cls[c];
+    if (cp.items.empty()) continue;
+    uint64_t q = 0;
+    for (size_t k = 0; k < cp.items.size(); ++k) {
+      const uint32_t i = cp.items[k];
+      Control *ctl = reinterpret_cast<Control *>(b->mem + (uint64_t)i * kCtlBytes);
+      if (c < 2) fill_ditem<float>(reinterpret_cast<DItem<float> *>(H(cp.table_off))[k], items[i], ctl);
+      else fill_ditem<double>(reinterpret_cast<DItem<double> *>(H(cp.table_off))[k], items[i], ctl);
+      const uint64_t G = (items[i].n + kChunk - 1) / kChunk;
+      unsigned long long *map = reinterpret_cast<unsigned long long *>(H(cp.map_off));
+      for (uint64_t ch = 0; ch < G; ++ch) map[q++] = ((unsigned long long)k << kBatchLocalBits) | ch;
+    }
+    switch (c) {
+      case 0: cp.grid = dec_grid<float, 2>(cp.chunks); break;
+      case 1: cp.grid = dec_grid<float, 3>(cp.chunks); break;
+      case 2: cp.grid = dec_grid<double, 2>(cp.chunks); break;
+      default: cp.grid = dec_grid<double, 3>(cp.chunks); break;
+    }
+    if (cp.grid < 1) {
+      cudaFree(b->mem);
+      delete b;
+      return GPZ_ECUDA;
+    }
+  }
+  if (cudaMemcpy(b->mem + b->zero_bytes, host.data(), host.size(), cudaMemcpyHostToDevice) != cudaSuccess) {
+    cudaFree(b->mem);
+    delete b;
+    return GPZ_ECUDA;
+  }
+  cudaStream_t s0 = nullptr;
+  cudaGraph_t graph = nullptr;
+  bool okc = cudaStreamCreateWithFlags(&s0, cudaStreamNonBlocking) == cudaSuccess;
+  if (okc) okc = cudaStreamBeginCapture(s0, cudaStreamCaptureModeThreadLocal) == cudaSuccess;
+  if (okc) {
+    cudaMemsetAsync(b->mem, 0, b->zero_bytes, s0);
+    for (int c = 0; c < 4; ++c) {  // one class after another, as in the compress graph
+      if (cls[c].items.empty()) continue;
+      switch (c) {
+        case 0: enqueue_dclass<float, 2>(cls[c], b->mem, s0); break;
+        case 1: enqueue_dclass<float, 3>(cls[c], b->mem, s0); break;
+        case 2: enqueue_dclass<double, 2>(cls[c], b->mem, s0); break;
+        default: enqueue_dclass<double, 3>(cls[c], b->mem, s0); break;
+      }
+    }
+    okc = cudaStreamEndCapture(s0, &graph) == cudaSuccess && graph;
+  }
+  if (okc) okc = cudaGraphInstantiate(&b->exec, graph, 0) == cudaSuccess;
+  if (graph) cudaGraphDestroy(graph);
+  if (s0) cudaStreamDestroy(s0);
+  if (!okc) {
+    cudaGetLastError();
+    cudaFree(b->mem);
+    delete b;
+    return GPZ_ECUDA;
+  }
+  *batch = b;
+  return GPZ_OK;
+}
+
+int gpz_dbatch_launch(gpz_dbatch *b, void *stream) {
+  if (!b || !b->exec) return GPZ_EINVAL;
+  return cudaGraphLaunch(b->exec, static_cast<cudaStream_t>(stream)) == cudaSuccess ? GPZ_OK : GPZ_ECUDA;
+}
+
+int gpz_dbatch_results(gpz_dbatch *b, gpz_result *results, void *stream) {
+  if (!b || !results) return GPZ_EINVAL;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  std::vector<Control> h(b->count);
+  for (uint32_t i = 0; i < b->count; ++i)
+    if (cudaMemcpyAsync(&h[i], b->mem + (uint64_t)i * kCtlBytes, sizeof(Control), cudaMemcpyDeviceToHost, st) !=
+        cudaSuccess)
+      return GPZ_ECUDA;
+  if (cudaStreamSynchronize(st) != cudaSuccess) return GPZ_ECUDA;
+  for (uint32_t i = 0; i < b->count; ++i) {
+    memset(&results[i], 0, sizeof(gpz_result));
+    results[i].status = h[i].status;
+  }
+  return GPZ_OK;
+}
+
+int gpz_dbatch_destroy(gpz_dbatch *b) {
   if (!b) return GPZ_EINVAL;
   if (b->exec) cudaGraphExecDestroy(b->exec);
   if (b->mem) cudaFree(b->mem);

@@ -312,14 +312,281 @@ __device__ __forceinline__ void scatter_runs(const uint32_t (&q)[N], const uint3
   }
 }
 
+// One chunk of a stream: c its index, n/G/pay_base/eb/seg from the validated
+// header, mwc the lanes' words of its meta record (dec_meta_word).  A record
+// or payload that fails validation sets GPZ_ESTREAM and writes nothing.
 template <typename T, int DIM>
-__global__ void __launch_bounds__(32 * DecCfg<T>::warps, DecCfg<T>::min_ctas) decompress_kernel(const DArgs<T> a) {
+__device__ __forceinline__ void decode_chunk(const DArgs<T> &a, unsigned long long c, unsigned long long n,
+                                             unsigned long long G, unsigned long long pay_base, T eb, uint32_t seg,
+                                             ChunkGeom &g, uint32_t mwc, uint32_t *sw, int lane) {
   using Tr = TT<T>;
   using Cfg = DecCfg<T>;
   using Acc = typename TT<T>::U;
   constexpr bool is64 = sizeof(T) == 8;
-  constexpr int W = Cfg::warps;
   constexpr uint32_t FULL = 0xFFFFFFFFu;
+  Control *ctl = a.ctl;
+  T *const Y[3] = {a.x, a.y, a.z};
+  const unsigned long long base = c * kChunk;
+  const uint32_t nvalid = (uint32_t)min((unsigned long long)kChunk, n - base);
+
+  // ---- chunk record: min/max, first id, bit widths, U, payload offset ----
+  T mm[6];
+  unsigned long long first, off;
+  uint32_t dbits, cbits, rbits, U;
+  if (!is64) {
+#pragma unroll
+    for (int k = 0; k < 6; ++k) mm[k] = (T)__uint_as_float(__shfl_sync(FULL, mwc, k));
+    first = __shfl_sync(FULL, mwc, 6);
+    const uint32_t w7 = __shfl_sync(FULL, mwc, 7), w8 = __shfl_sync(FULL, mwc, 8);
+    dbits = w7 & 0xFFFFu; cbits = w7 >> 16; rbits = w8 & 0xFFFFu; U = w8 >> 16;
+    off = __shfl_sync(FULL, mwc, 9) | ((unsigned long long)__shfl_sync(FULL, mwc, 10) << 32);
+  } else {
+#pragma unroll
+    for (int k = 0; k < 6; ++k)
+      mm[k] = (T)__hiloint2double((int)__shfl_sync(FULL, mwc, 2 * k + 1), (int)__shfl_sync(FULL, mwc, 2 * k));
+    first = __shfl_sync(FULL, mwc, 12) | ((unsigned long long)__shfl_sync(FULL, mwc, 13) << 32);
+    const uint32_t w14 = __shfl_sync(FULL, mwc, 14), w15 = __shfl_sync(FULL, mwc, 15);
+    dbits = w14 & 0xFFFFu; cbits = w14 >> 16; rbits = w15 & 0xFFFFu; U = w15 >> 16;
+    off = __shfl_sync(FULL, mwc, 16) | ((unsigned long long)__shfl_sync(FULL, mwc, 17) << 32);
+  }
+  const uint32_t db = section_bytes(U, dbits, Tr::pad), cb = section_bytes(U, cbits, Tr::pad);
+  const uint32_t rb = rel_section_bytes(rbits, Tr::pad);
+  const unsigned long long pl = (unsigned long long)db + cb + rb;
+  const bool ok = U >= 1 && U <= nvalid && dbits <= 32 && cbits <= 32 && rbits <= 32 && (off & (Tr::pad)) == 0 &&
+                  pl <= (unsigned long long)kStageBytes && pay_base <= a.bytes && off <= a.bytes - pay_base &&
+                  pl <= a.bytes - pay_base - off;
+  if (!ok) {
+    if (lane == 0) set_status(ctl, kESTREAM);
+    return;
+  }
+  const uint32_t *pw = reinterpret_cast<const uint32_t *>(a.s + pay_base + off);
+  const uint32_t bpp = (U + 7u) >> 3;
+  const uint32_t endd = db >> 2, endc = (db + cb) >> 2;  // section end words
+
+  // all plane words of the usual section widths in flight at once
+  PlaneWords<8, true> rawc;
+  PlaneWords<16, true> rawd;
+  PlaneWords<16, false> rawr;
+  rawc.load(pw, db, cbits, bpp, endc, lane);
+  rawd.load(pw, 0u, dbits, bpp, endd, lane);
+  rawr.load(pw, db + cb, rbits, 0u, 0u, lane);
+
+  // valid elements of this lane's unit; delta 0 is replaced by the first id
+  const int nl_i = min(max((int)U - 32 * lane, 0), 32);
+  const uint32_t nl = (uint32_t)nl_i;
+  const uint32_t vm = nl >= 32u ? FULL : ((1u << nl) - 1u);
+  const uint32_t vmd = lane == 0 ? (vm & ~1u) : vm;
+
+  // block counts (:831-837 / Double :835-838); lanes 0..2 build the three
+  // dividers at once
+  const T rx = is64 ? (T)__dsub_rn((double)mm[3], (double)mm[0]) : (T)__fsub_rn((float)mm[3], (float)mm[0]);
+  const T ry = is64 ? (T)__dsub_rn((double)mm[4], (double)mm[1]) : (T)__fsub_rn((float)mm[4], (float)mm[1]);
+  const unsigned long long bnx = block_num(rx, seg, eb, false), bny = block_num(ry, seg, eb, false);
+  g.bnx = (uint32_t)bnx;
+  g.bny = (uint32_t)bny;
+  g.bnx64 = bnx;
+  g.bny64 = bny;
+  g.wide = is64 && ((bnx >> 32) != 0 || (bny >> 32) != 0 || ((bnx * bny) >> 32) != 0);
+  const uint32_t my_div = lane == 0 ? (uint32_t)bnx : (lane == 1 ? (uint32_t)bny : (uint32_t)(bnx * bny));
+  {
+    FastDiv31 d31;
+    d31.init(my_div);
+    g.gx.d = __shfl_sync(FULL, d31.d, 0); g.gx.m = __shfl_sync(FULL, d31.m, 0); g.gx.l = __shfl_sync(FULL, d31.l, 0);
+    g.gy.d = __shfl_sync(FULL, d31.d, 1); g.gy.m = __shfl_sync(FULL, d31.m, 1); g.gy.l = __shfl_sync(FULL, d31.l, 1);
+  }
+  uint32_t *const A = sw + Cfg::A;
+#pragma unroll
+  for (int m = 0; m < 8; ++m) reinterpret_cast<uint4 *>(A + 32 * lane)[m] = make_uint4(0u, 0u, 0u, 0u);
+
+  // ---- counts -> run starts as 16-bit pairs P16[k] = st_k | st_{k+16} << 16 ----
+  uint32_t P16[16];
+  bool bad = false;
+  {
+    uint32_t orw = 0;
+    if (cbits <= 8u) {
+      uint32_t q[8];
+      section_words<8>(q, rawc, pw, db, cbits, bpp, endc, vm, lane, orw);
+#pragma unroll
+      for (int k = 0; k < 8; ++k) {
+        P16[k] = prmt(q[k], 0u, 0x4240);
+        P16[k + 8] = prmt(q[k], 0u, 0x4341);
+      }
+    } else if (cbits <= 16u) {
+      uint32_t q[16];
+      section_words<16>(q, rawc, pw, db, cbits, bpp, endc, vm, lane, orw);
+#pragma unroll
+      for (int k = 0; k < 16; ++k) {
+        bad |= (q[k] & 0xFFFFu) > (uint32_t)kChunk || (q[k] >> 16) > (uint32_t)kChunk;
+        P16[k] = q[k];
+      }
+    } else {
+      uint32_t q[32];
+      section_words<32>(q, rawc, pw, db, cbits, bpp, endc, vm, lane, orw);
+#pragma unroll
+      for (int k = 0; k < 16; ++k) {
+        bad |= q[k] > (uint32_t)kChunk || q[k + 16] > (uint32_t)kChunk;
+        P16[k] = (q[k] & 0xFFFFu) | (q[k + 16] << 16);
+      }
+    }
+    // every run holds 1..1024 points (8-bit counts cannot exceed 1024)
+    bad |= (orw & vm) != vm;  // a zero count
+    uint32_t run = 0;
+#pragma unroll
+    for (int k = 0; k < 16; ++k) {
+      const uint32_t v = P16[k];
+      P16[k] = run;
+      run += v;
+    }
+    const uint32_t s_lo = run & 0xFFFFu, loc = s_lo + (run >> 16);
+    uint32_t inc = loc;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t t = __shfl_up_sync(FULL, inc, o);
+      if (lane >= o) inc += t;
+    }
+    if (__any_sync(FULL, bad) || __shfl_sync(FULL, inc, 31) != nvalid) {
+      if (lane == 0) set_status(ctl, kESTREAM);
+      return;
+    }
+    const uint32_t cbase = inc - loc, add = cbase | ((cbase + s_lo) << 16);
+#pragma unroll
+    for (int k = 0; k < 16; ++k) P16[k] += add;
+  }
+  __syncwarp();  // run map rows cleared
+
+  // ---- deltas -> ids: id[0] = first, id[u] = id[u-1] + delta[u] (:930-938) ----
+  bool fast = false;
+  {
+    auto run_ids = [&](auto &q) {
+      constexpr int N = sizeof(q) / sizeof(uint32_t);
+      Acc loc = 0;
+      if constexpr (N == 8) {
+        uint32_t t = 0;
+#pragma unroll
+        for (int k = 0; k < 8; ++k) t = __dp4a(q[k], 0x01010101u, t);
+        loc = t;
+      } else if constexpr (N == 16) {
+        uint32_t t = 0;
+#pragma unroll
+        for (int k = 0; k < 16; ++k) t = __dp2a_lo(q[k], 0x0101u, t);
+        loc = t;
+      } else {
+#pragma unroll
+        for (int k = 0; k < 32; ++k) loc += (Acc)q[k];
+      }
+      Acc inc = loc;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const Acc t = __shfl_up_sync(FULL, inc, o);
+        if (lane >= o) inc += t;
+      }
+      // the last id bounds them all (ids never decrease); 1023 deltas below
+      // 2^21 cannot wrap a 32-bit sum
+      const unsigned long long total = (unsigned long long)__shfl_sync(FULL, inc, 31);
+      fast = dbits <= 21u && first + total < (1ull << 31) && !g.wide && bnx != 0 && bny != 0 &&
+             bnx * bny < (1ull << 32);
+      scatter_runs<T, N>(q, P16, sw, (Acc)first + (inc - loc), nl, fast, lane);
+    };
+    uint32_t orw = 0;
+    if (dbits <= 8u) {
+      uint32_t q[8];
+      section_words<8>(q, rawd, pw, 0u, dbits, bpp, endd, vmd, lane, orw);
+      run_ids(q);
+    } else if (dbits <= 16u) {
+      uint32_t q[16];
+      section_words<16>(q, rawd, pw, 0u, dbits, bpp, endd, vmd, lane, orw);
+      run_ids(q);
+    } else {
+      uint32_t q[32];
+      section_words<32>(q, rawd, pw, 0u, dbits, bpp, endd, vmd, lane, orw);
+      run_ids(q);
+    }
+  }
+  __syncwarp();
+
+  // ---- every position's id (or run): inclusive max-scan of the run map ----
+  {
+    uint32_t v[32];
+    uint32_t mx = 0;
+#pragma unroll
+    for (int m = 0; m < 8; ++m) {
+      const uint4 t = *reinterpret_cast<const uint4 *>(A + qoff(lane, m));
+      mx = max(mx, t.x); v[4 * m] = mx;
+      mx = max(mx, t.y); v[4 * m + 1] = mx;
+      mx = max(mx, t.z); v[4 * m + 2] = mx;
+      mx = max(mx, t.w); v[4 * m + 3] = mx;
+    }
+    uint32_t inc = mx;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t t = __shfl_up_sync(FULL, inc, o);
+      if (lane >= o) inc = max(inc, t);
+    }
+    uint32_t pre = __shfl_up_sync(FULL, inc, 1);
+    if (lane == 0) pre = 0;
+    uint32_t *const P = sw + Cfg::P;
+    const uint32_t *const TL = sw + Cfg::TL;
+    const bool gather = !is64 && !fast;  // float general path: run index -> 32-bit id
+#pragma unroll
+    for (int m = 0; m < 8; ++m) {
+      uint32_t o[4];
+#pragma unroll
+      for (int e = 0; e < 4; ++e) {
+        const uint32_t r = max(v[4 * m + e], pre);
+        o[e] = gather ? TL[swz((int)r)] : r;
+      }
+      *reinterpret_cast<uint4 *>(P + qoff(lane, m)) = make_uint4(o[0], o[1], o[2], o[3]);
+    }
+  }
+  __syncwarp();  // the float id table becomes the relative-position rows
+
+  // ---- relative positions of this lane's 32 positions ----
+  {
+    uint32_t *const R = sw + Cfg::R;
+    uint32_t orw = 0;
+    auto put = [&](auto &q) {
+      constexpr int N = sizeof(q) / sizeof(uint32_t);
+#pragma unroll
+      for (int m = 0; m < 8; ++m)
+        *reinterpret_cast<uint4 *>(R + qoff(lane, m)) =
+            make_uint4(word_value<N>(q, 4 * m), word_value<N>(q, 4 * m + 1), word_value<N>(q, 4 * m + 2),
+                       word_value<N>(q, 4 * m + 3));
+    };
+    if (rbits <= 8u) {
+      uint32_t q[8];
+      section_words<8>(q, rawr, pw, db + cb, rbits, 0u, 0u, FULL, lane, orw);
+      put(q);
+    } else if (rbits <= 16u) {
+      uint32_t q[16];
+      section_words<16>(q, rawr, pw, db + cb, rbits, 0u, 0u, FULL, lane, orw);
+      put(q);
+    } else {
+      uint32_t q[32];
+      section_words<32>(q, rawr, pw, db + cb, rbits, 0u, 0u, FULL, lane, orw);
+      put(q);
+    }
+  }
+
+  // ---- reconstruct ----
+  const bool full = nvalid == (uint32_t)kChunk && a.vec_ok;
+  if (fast) {
+    reconstruct<T, DIM, 0>(sw, g, eb, mm, Y, base, lane, nvalid, full);
+  } else {
+    FastDiv f;
+    f.init(my_div);
+    g.fx.d = __shfl_sync(FULL, f.d, 0); g.fx.m = __shfl_sync(FULL, f.m, 0); g.fx.s = __shfl_sync(FULL, f.s, 0);
+    g.fy.d = __shfl_sync(FULL, f.d, 1); g.fy.m = __shfl_sync(FULL, f.m, 1); g.fy.s = __shfl_sync(FULL, f.s, 1);
+    g.fxy.d = __shfl_sync(FULL, f.d, 2); g.fxy.m = __shfl_sync(FULL, f.m, 2); g.fxy.s = __shfl_sync(FULL, f.s, 2);
+    if constexpr (!is64) reconstruct<T, DIM, 1>(sw, g, eb, mm, Y, base, lane, nvalid, full);
+    else reconstruct<T, DIM, 2>(sw, g, eb, mm, Y, base, lane, nvalid, full);
+  }
+}
+
+template <typename T, int DIM>
+__global__ void __launch_bounds__(32 * DecCfg<T>::warps, DecCfg<T>::min_ctas) decompress_kernel(const DArgs<T> a) {
+  using Tr = TT<T>;
+  using Cfg = DecCfg<T>;
+  constexpr int W = Cfg::warps;
   extern __shared__ __align__(16) uint32_t dec_smem[];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   uint32_t *const sw = dec_smem + warp * Cfg::words;
@@ -341,7 +608,6 @@ __global__ void __launch_bounds__(32 * DecCfg<T>::warps, DecCfg<T>::min_ctas) de
   }
   if (n > a.cap) { if (threadIdx.x == 0) set_status(ctl, kENOSPACE); return; }
   const unsigned long long pay_base = Tr::hdr + 8ull * G + (unsigned long long)Tr::meta * G;
-  T *const Y[3] = {a.x, a.y, a.z};
   const unsigned long long nwarps = (unsigned long long)gridDim.x * W;
   ChunkGeom g;
   g.seg = seg;
@@ -353,260 +619,7 @@ __global__ void __launch_bounds__(32 * DecCfg<T>::warps, DecCfg<T>::min_ctas) de
   for (; c < G; c += nwarps) {
     const uint32_t mwc = mw;
     if (c + nwarps < G) mw = dec_meta_word<T>(a.s, G, c + nwarps, lane);  // next record, in flight meanwhile
-    const unsigned long long base = c * kChunk;
-    const uint32_t nvalid = (uint32_t)min((unsigned long long)kChunk, n - base);
-
-    // ---- chunk record: min/max, first id, bit widths, U, payload offset ----
-    T mm[6];
-    unsigned long long first, off;
-    uint32_t dbits, cbits, rbits, U;
-    if (!is64) {
-#pragma unroll
-      for (int k = 0; k < 6; ++k) mm[k] = (T)__uint_as_float(__shfl_sync(FULL, mwc, k));
-      first = __shfl_sync(FULL, mwc, 6);
-      const uint32_t w7 = __shfl_sync(FULL, mwc, 7), w8 = __shfl_sync(FULL, mwc, 8);
-      dbits = w7 & 0xFFFFu; cbits = w7 >> 16; rbits = w8 & 0xFFFFu; U = w8 >> 16;
-      off = __shfl_sync(FULL, mwc, 9) | ((unsigned long long)__shfl_sync(FULL, mwc, 10) << 32);
-    } else {
-#pragma unroll
-      for (int k = 0; k < 6; ++k)
-        mm[k] = (T)__hiloint2double((int)__shfl_sync(FULL, mwc, 2 * k + 1), (int)__shfl_sync(FULL, mwc, 2 * k));
-      first = __shfl_sync(FULL, mwc, 12) | ((unsigned long long)__shfl_sync(FULL, mwc, 13) << 32);
-      const uint32_t w14 = __shfl_sync(FULL, mwc, 14), w15 = __shfl_sync(FULL, mwc, 15);
-      dbits = w14 & 0xFFFFu; cbits = w14 >> 16; rbits = w15 & 0xFFFFu; U = w15 >> 16;
-      off = __shfl_sync(FULL, mwc, 16) | ((unsigned long long)__shfl_sync(FULL, mwc, 17) << 32);
-    }
-    const uint32_t db = section_bytes(U, dbits, Tr::pad), cb = section_bytes(U, cbits, Tr::pad);
-    const uint32_t rb = rel_section_bytes(rbits, Tr::pad);
-    const unsigned long long pl = (unsigned long long)db + cb + rb;
-    const bool ok = U >= 1 && U <= nvalid && dbits <= 32 && cbits <= 32 && rbits <= 32 && (off & (Tr::pad)) == 0 &&
-                    pl <= (unsigned long long)kStageBytes && pay_base <= a.bytes && off <= a.bytes - pay_base &&
-                    pl <= a.bytes - pay_base - off;
-    if (!ok) {
-      if (lane == 0) set_status(ctl, kESTREAM);
-      continue;
-    }
-    const uint32_t *pw = reinterpret_cast<const uint32_t *>(a.s + pay_base + off);
-    const uint32_t bpp = (U + 7u) >> 3;
-    const uint32_t endd = db >> 2, endc = (db + cb) >> 2;  // section end words
-
-    // all plane words of the usual section widths in flight at once
-    PlaneWords<8, true> rawc;
-    PlaneWords<16, true> rawd;
-    PlaneWords<16, false> rawr;
-    rawc.load(pw, db, cbits, bpp, endc, lane);
-    rawd.load(pw, 0u, dbits, bpp, endd, lane);
-    rawr.load(pw, db + cb, rbits, 0u, 0u, lane);
-
-    // valid elements of this lane's unit; delta 0 is replaced by the first id
-    const int nl_i = min(max((int)U - 32 * lane, 0), 32);
-    const uint32_t nl = (uint32_t)nl_i;
-    const uint32_t vm = nl >= 32u ? FULL : ((1u << nl) - 1u);
-    const uint32_t vmd = lane == 0 ? (vm & ~1u) : vm;
-
-    // block counts (:831-837 / Double :835-838); lanes 0..2 build the three
-    // dividers at once
-    const T rx = is64 ? (T)__dsub_rn((double)mm[3], (double)mm[0]) : (T)__fsub_rn((float)mm[3], (float)mm[0]);
-    const T ry = is64 ? (T)__dsub_rn((double)mm[4], (double)mm[1]) : (T)__fsub_rn((float)mm[4], (float)mm[1]);
-    const unsigned long long bnx = block_num(rx, seg, eb, false), bny = block_num(ry, seg, eb, false);
-    g.bnx = (uint32_t)bnx;
-    g.bny = (uint32_t)bny;
-    g.bnx64 = bnx;
-    g.bny64 = bny;
-    g.wide = is64 && ((bnx >> 32) != 0 || (bny >> 32) != 0 || ((bnx * bny) >> 32) != 0);
-    const uint32_t my_div = lane == 0 ? (uint32_t)bnx : (lane == 1 ? (uint32_t)bny : (uint32_t)(bnx * bny));
-    {
-      FastDiv31 d31;
-      d31.init(my_div);
-      g.gx.d = __shfl_sync(FULL, d31.d, 0); g.gx.m = __shfl_sync(FULL, d31.m, 0); g.gx.l = __shfl_sync(FULL, d31.l, 0);
-      g.gy.d = __shfl_sync(FULL, d31.d, 1); g.gy.m = __shfl_sync(FULL, d31.m, 1); g.gy.l = __shfl_sync(FULL, d31.l, 1);
-    }
-    uint32_t *const A = sw + Cfg::A;
-#pragma unroll
-    for (int m = 0; m < 8; ++m) reinterpret_cast<uint4 *>(A + 32 * lane)[m] = make_uint4(0u, 0u, 0u, 0u);
-
-    // ---- counts -> run starts as 16-bit pairs P16[k] = st_k | st_{k+16} << 16 ----
-    uint32_t P16[16];
-    bool bad = false;
-    {
-      uint32_t orw = 0;
-      if (cbits <= 8u) {
-        uint32_t q[8];
-        section_words<8>(q, rawc, pw, db, cbits, bpp, endc, vm, lane, orw);
-#pragma unroll
-        for (int k = 0; k < 8; ++k) {
-          P16[k] = prmt(q[k], 0u, 0x4240);
-          P16[k + 8] = prmt(q[k], 0u, 0x4341);
-        }
-      } else if (cbits <= 16u) {
-        uint32_t q[16];
-        section_words<16>(q, rawc, pw, db, cbits, bpp, endc, vm, lane, orw);
-#pragma unroll
-        for (int k = 0; k < 16; ++k) {
-          bad |= (q[k] & 0xFFFFu) > (uint32_t)kChunk || (q[k] >> 16) > (uint32_t)kChunk;
-          P16[k] = q[k];
-        }
-      } else {
-        uint32_t q[32];
-        section_words<32>(q, rawc, pw, db, cbits, bpp, endc, vm, lane, orw);
-#pragma unroll
-        for (int k = 0; k < 16; ++k) {
-          bad |= q[k] > (uint32_t)kChunk || q[k + 16] > (uint32_t)kChunk;
-          P16[k] = (q[k] & 0xFFFFu) | (q[k + 16] << 16);
-        }
-      }
-      // every run holds 1..1024 points (8-bit counts cannot exceed 1024)
-      bad |= (orw & vm) != vm;  // a zero count
-      uint32_t run = 0;
-#pragma unroll
-      for (int k = 0; k < 16; ++k) {
-        const uint32_t v = P16[k];
-        P16[k] = run;
-        run += v;
-      }
-      const uint32_t s_lo = run & 0xFFFFu, loc = s_lo + (run >> 16);
-      uint32_t inc = loc;
-#pragma unroll
-      for (int o = 1; o < 32; o <<= 1) {
-        const uint32_t t = __shfl_up_sync(FULL, inc, o);
-        if (lane >= o) inc += t;
-      }
-      if (__any_sync(FULL, bad) || __shfl_sync(FULL, inc, 31) != nvalid) {
-        if (lane == 0) set_status(ctl, kESTREAM);
-        continue;
-      }
-      const uint32_t cbase = inc - loc, add = cbase | ((cbase + s_lo) << 16);
-#pragma unroll
-      for (int k = 0; k < 16; ++k) P16[k] += add;
-    }
-    __syncwarp();  // run map rows cleared
-
-    // ---- deltas -> ids: id[0] = first, id[u] = id[u-1] + delta[u] (:930-938) ----
-    bool fast = false;
-    {
-      auto run_ids = [&](auto &q) {
-        constexpr int N = sizeof(q) / sizeof(uint32_t);
-        Acc loc = 0;
-        if constexpr (N == 8) {
-          uint32_t t = 0;
-#pragma unroll
-          for (int k = 0; k < 8; ++k) t = __dp4a(q[k], 0x01010101u, t);
-          loc = t;
-        } else if constexpr (N == 16) {
-          uint32_t t = 0;
-#pragma unroll
-          for (int k = 0; k < 16; ++k) t = __dp2a_lo(q[k], 0x0101u, t);
-          loc = t;
-        } else {
-#pragma unroll
-          for (int k = 0; k < 32; ++k) loc += (Acc)q[k];
-        }
-        Acc inc = loc;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-          const Acc t = __shfl_up_sync(FULL, inc, o);
-          if (lane >= o) inc += t;
-        }
-        // the last id bounds them all (ids never decrease); 1023 deltas below
-        // 2^21 cannot wrap a 32-bit sum
-        const unsigned long long total = (unsigned long long)__shfl_sync(FULL, inc, 31);
-        fast = dbits <= 21u && first + total < (1ull << 31) && !g.wide && bnx != 0 && bny != 0 &&
-               bnx * bny < (1ull << 32);
-        scatter_runs<T, N>(q, P16, sw, (Acc)first + (inc - loc), nl, fast, lane);
-      };
-      uint32_t orw = 0;
-      if (dbits <= 8u) {
-        uint32_t q[8];
-        section_words<8>(q, rawd, pw, 0u, dbits, bpp, endd, vmd, lane, orw);
-        run_ids(q);
-      } else if (dbits <= 16u) {
-        uint32_t q[16];
-        section_words<16>(q, rawd, pw, 0u, dbits, bpp, endd, vmd, lane, orw);
-        run_ids(q);
-      } else {
-        uint32_t q[32];
-        section_words<32>(q, rawd, pw, 0u, dbits, bpp, endd, vmd, lane, orw);
-        run_ids(q);
-      }
-    }
-    __syncwarp();
-
-    // ---- every position's id (or run): inclusive max-scan of the run map ----
-    {
-      uint32_t v[32];
-      uint32_t mx = 0;
-#pragma unroll
-      for (int m = 0; m < 8; ++m) {
-        const uint4 t = *reinterpret_cast<const uint4 *>(A + qoff(lane, m));
-        mx = max(mx, t.x); v[4 * m] = mx;
-        mx = max(mx, t.y); v[4 * m + 1] = mx;
-        mx = max(mx, t.z); v[4 * m + 2] = mx;
-        mx = max(mx, t.w); v[4 * m + 3] = mx;
-      }
-      uint32_t inc = mx;
-#pragma unroll
-      for (int o = 1; o < 32; o <<= 1) {
-        const uint32_t t = __shfl_up_sync(FULL, inc, o);
-        if (lane >= o) inc = max(inc, t);
-      }
-      uint32_t pre = __shfl_up_sync(FULL, inc, 1);
-      if (lane == 0) pre = 0;
-      uint32_t *const P = sw + Cfg::P;
-      const uint32_t *const TL = sw + Cfg::TL;
-      const bool gather = !is64 && !fast;  // float general path: run index -> 32-bit id
-#pragma unroll
-      for (int m = 0; m < 8; ++m) {
-        uint32_t o[4];
-#pragma unroll
-        for (int e = 0; e < 4; ++e) {
-          const uint32_t r = max(v[4 * m + e], pre);
-          o[e] = gather ? TL[swz((int)r)] : r;
-        }
-        *reinterpret_cast<uint4 *>(P + qoff(lane, m)) = make_uint4(o[0], o[1], o[2], o[3]);
-      }
-    }
-    __syncwarp();  // the float id table becomes the relative-position rows
-
-    // ---- relative positions of this lane's 32 positions ----
-    {
-      uint32_t *const R = sw + Cfg::R;
-      uint32_t orw = 0;
-      auto put = [&](auto &q) {
-        constexpr int N = sizeof(q) / sizeof(uint32_t);
-#pragma unroll
-        for (int m = 0; m < 8; ++m)
-          *reinterpret_cast<uint4 *>(R + qoff(lane, m)) =
-              make_uint4(word_value<N>(q, 4 * m), word_value<N>(q, 4 * m + 1), word_value<N>(q, 4 * m + 2),
-                         word_value<N>(q, 4 * m + 3));
-      };
-      if (rbits <= 8u) {
-        uint32_t q[8];
-        section_words<8>(q, rawr, pw, db + cb, rbits, 0u, 0u, FULL, lane, orw);
-        put(q);
-      } else if (rbits <= 16u) {
-        uint32_t q[16];
-        section_words<16>(q, rawr, pw, db + cb, rbits, 0u, 0u, FULL, lane, orw);
-        put(q);
-      } else {
-        uint32_t q[32];
-        section_words<32>(q, rawr, pw, db + cb, rbits, 0u, 0u, FULL, lane, orw);
-        put(q);
-      }
-    }
-
-    // ---- reconstruct ----
-    const bool full = nvalid == (uint32_t)kChunk && a.vec_ok;
-    if (fast) {
-      reconstruct<T, DIM, 0>(sw, g, eb, mm, Y, base, lane, nvalid, full);
-    } else {
-      FastDiv f;
-      f.init(my_div);
-      g.fx.d = __shfl_sync(FULL, f.d, 0); g.fx.m = __shfl_sync(FULL, f.m, 0); g.fx.s = __shfl_sync(FULL, f.s, 0);
-      g.fy.d = __shfl_sync(FULL, f.d, 1); g.fy.m = __shfl_sync(FULL, f.m, 1); g.fy.s = __shfl_sync(FULL, f.s, 1);
-      g.fxy.d = __shfl_sync(FULL, f.d, 2); g.fxy.m = __shfl_sync(FULL, f.m, 2); g.fxy.s = __shfl_sync(FULL, f.s, 2);
-      if constexpr (!is64) reconstruct<T, DIM, 1>(sw, g, eb, mm, Y, base, lane, nvalid, full);
-      else reconstruct<T, DIM, 2>(sw, g, eb, mm, Y, base, lane, nvalid, full);
-    }
+    decode_chunk<T, DIM>(a, c, n, G, pay_base, eb, seg, g, mwc, sw, lane);
   }
 }
 

@@ -277,6 +277,33 @@ int gpz_batch_results(gpz_batch *batch, gpz_result *results, double *h_eb, void 
 uint64_t gpz_batch_device_bytes(const gpz_batch *batch);
 int gpz_batch_destroy(gpz_batch *batch);
 
+/* ---- batched decompress ------------------------------------------------------------
+ * No counterpart in the reference (one stream per CompressorManager::decompressWarp
+ * call, src/CompressorManager.cpp:18-22).  Many streams of mixed float width
+ * and dimension decoded by one CUDA graph: a header check per stream, then one
+ * persistent decompress kernel per class whose warps stride over the chunks of
+ * all its streams.  Each stream's output equals gpz_decompress's.  Same plan
+ * model as gpz_batch: bound to the buffers at creation, launched any number of
+ * times, launches must not overlap. */
+typedef struct gpz_dbatch_item {
+  const void *d_stream;  /* the stream on the device */
+  uint64_t stream_bytes;
+  uint32_t float_bits;   /* from the stream header (gpz_parse_header on a host copy) */
+  uint32_t dim;
+  uint64_t n;            /* points, from the stream header; checked on the device */
+  void *d_x;             /* SoA outputs, out_capacity points each; d_z ignored for 2D */
+  void *d_y;
+  void *d_z;
+  uint64_t out_capacity;
+} gpz_dbatch_item;
+
+typedef struct gpz_dbatch gpz_dbatch;
+
+int gpz_dbatch_create(const gpz_dbatch_item *items, uint32_t count, gpz_dbatch **batch, uint32_t *bad_item);
+int gpz_dbatch_launch(gpz_dbatch *batch, void *stream);
+int gpz_dbatch_results(gpz_dbatch *batch, gpz_result *results, void *stream);
+int gpz_dbatch_destroy(gpz_dbatch *batch);
+
 /* Library version string. */
 const char *gpz_version(void);
 

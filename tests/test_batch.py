@@ -127,3 +127,72 @@ def test_batch_reports_a_failed_snapshot_and_finishes_the_others():
         assert b.snapshots[2].out[: res[2][0].stream_bytes].cpu().numpy().tobytes() == want
     finally:
         b.close()
+
+
+@pytest.mark.gpu
+def test_decompress_batch_equals_single_calls():
+    """The batch's streams decoded by one DecompressBatch launch equal
+    gz.decompress of each stream, bit for bit, on two launches; a corrupted
+    stream in the batch reports GPZ_ESTREAM without disturbing the others."""
+    import torch
+    from gpz_b200.batch import Batch, DecompressBatch, Snapshot
+    snaps = _mixed_snapshots()
+    b = Batch([Snapshot(x, y, z, **kw) for x, y, z, kw in snaps])
+    try:
+        b.launch()
+        streams = [t.clone() for t in b.streams()]
+    finally:
+        b.close()
+    bad = streams[4].clone()
+    hb = 24
+    G = (snaps[4][0].numel() + 1023) // 1024
+    bad[hb + 8 * G + 36 * 1 + 34] = 0xFF  # chunk 1's U field: impossible
+    bad[hb + 8 * G + 36 * 1 + 35] = 0xFF
+    d = DecompressBatch(streams + [bad])
+    try:
+        for _ in range(2):
+            for o in d.outputs:
+                for t in o:
+                    if t is not None:
+                        t.fill_(-1.0)
+            d.launch()
+            st = d.results()
+            assert st[:-1] == [0] * len(streams) and st[-1] == gz.GPZ_ESTREAM
+            for s, o in zip(streams, d.outputs):
+                want = gz.decompress(s)
+                for a, w in zip(o, want):
+                    if w is None:
+                        assert a is None
+                    else:
+                        assert torch.equal(a.view(torch.uint8), w.view(torch.uint8))
+    finally:
+        d.close()
+
+
+@pytest.mark.gpu
+def test_autotune_picks_the_smallest_sample_and_keeps_bytes_identical():
+    """The tuner's choice is the candidate with the smallest sample stream;
+    the batch compressed with the tuned segment sizes equals single calls with
+    the same fixed segment sizes."""
+    from gpz_b200.batch import Batch, Snapshot, autotune
+    snaps = _mixed_snapshots()[1:6]
+    snapshots = [Snapshot(x, y, z, **kw) for x, y, z, kw in snaps]
+    recs = autotune(snapshots, sample_points=20_000)
+    for s, rec, (x, y, z, kw) in zip(snapshots, recs, snaps):
+        if kw.get("seg_size") or kw.get("fixed"):
+            assert rec == {}
+            continue
+        assert rec["sample_bytes"] and s.fixed and s.seg_size == rec["seg"]
+        assert rec["sample_bytes"][rec["seg"]] == min(rec["sample_bytes"].values())
+    b = Batch(snapshots)
+    try:
+        b.launch()
+        res = b.results()
+        for s, (r, eb), (x, y, z, kw) in zip(snapshots, res, snaps):
+            bits = 32 if x.dtype.itemsize == 4 else 64
+            kw2 = dict(kw, seg_size=s.seg_size, fixed=True)
+            want, r1, eb1 = _single(x, y, z, kw2, bits)
+            assert r.status == 0 and eb == eb1 and r.seg_size == s.seg_size
+            assert s.out[: r.stream_bytes].cpu().numpy().tobytes() == want
+    finally:
+        b.close()
