@@ -27,6 +27,7 @@ GPZ_OK, GPZ_EINVAL, GPZ_ESEG, GPZ_ESTREAM, GPZ_ENOSPACE, GPZ_ECUDA, GPZ_ETIMEOUT
 GPZ_FLAG_SAFE31 = 1
 GPZ_FLAG_SEG_FIXED = 2
 GPZ_FLAG_REL_ON_DEVICE = 4
+GPZ_OP_COMPRESS, GPZ_OP_DECOMPRESS = 1, 2
 ERRORS = {1: "EINVAL", 2: "ESEG", 3: "ESTREAM", 4: "ENOSPACE", 5: "ECUDA", 6: "ETIMEOUT", 7: "ENOTSUP", 8: "ELIMIT"}
 
 
@@ -59,6 +60,32 @@ class BatchItem(ctypes.Structure):
                 ("d_out", ctypes.c_void_p), ("out_capacity", ctypes.c_uint64), ("eb", ctypes.c_double),
                 ("rel_eb", ctypes.c_double), ("rel_mode", ctypes.c_int32), ("seg_size", ctypes.c_uint32),
                 ("flags", ctypes.c_uint32), ("reserved", ctypes.c_uint32)]
+
+
+class ServerConfig(ctypes.Structure):
+    _fields_ = [("hbm_budget", ctypes.c_uint64), ("streams", ctypes.c_uint32), ("max_batch", ctypes.c_uint32),
+                ("workspace_bytes", ctypes.c_uint64)]
+
+
+class Request(ctypes.Structure):
+    """gpz_request: one compress or decompress request to a server."""
+    _fields_ = [("op", ctypes.c_uint32), ("float_bits", ctypes.c_uint32), ("dim", ctypes.c_uint32),
+                ("flags", ctypes.c_uint32), ("n", ctypes.c_uint64), ("d_x", ctypes.c_void_p),
+                ("d_y", ctypes.c_void_p), ("d_z", ctypes.c_void_p), ("d_stream", ctypes.c_void_p),
+                ("stream_bytes", ctypes.c_uint64), ("eb", ctypes.c_double), ("rel_eb", ctypes.c_double),
+                ("rel_mode", ctypes.c_int32), ("seg_size", ctypes.c_uint32)]
+
+
+class Completion(ctypes.Structure):
+    _fields_ = [("status", ctypes.c_int32), ("seg_size", ctypes.c_uint32), ("stream_bytes", ctypes.c_uint64),
+                ("d_out", ctypes.c_void_p), ("eb", ctypes.c_double), ("queue_ms", ctypes.c_double),
+                ("total_ms", ctypes.c_double), ("batch_size", ctypes.c_uint32), ("reserved", ctypes.c_uint32)]
+
+
+class ServerStats(ctypes.Structure):
+    _fields_ = [("submitted", ctypes.c_uint64), ("completed", ctypes.c_uint64), ("batches", ctypes.c_uint64),
+                ("arena_bytes", ctypes.c_uint64), ("arena_free_bytes", ctypes.c_uint64),
+                ("queued", ctypes.c_uint32), ("in_flight", ctypes.c_uint32)]
 
 
 class DBatchItem(ctypes.Structure):
@@ -107,6 +134,12 @@ SIGNATURES = {
     "gpz_dbatch_launch": (ctypes.c_int, [_VP, _VP]),
     "gpz_dbatch_results": (ctypes.c_int, [_VP, ctypes.POINTER(Result), _VP]),
     "gpz_dbatch_destroy": (ctypes.c_int, [_VP]),
+    "gpz_server_create": (ctypes.c_int, [ctypes.POINTER(ServerConfig), ctypes.POINTER(_VP)]),
+    "gpz_server_submit": (ctypes.c_int, [_VP, ctypes.POINTER(Request), ctypes.POINTER(_U64)]),
+    "gpz_server_wait": (ctypes.c_int, [_VP, _U64, ctypes.POINTER(Completion), _U32]),
+    "gpz_server_release": (ctypes.c_int, [_VP, _U64]),
+    "gpz_server_stats_get": (ctypes.c_int, [_VP, ctypes.POINTER(ServerStats)]),
+    "gpz_server_destroy": (ctypes.c_int, [_VP]),
 }
 
 _lib = None

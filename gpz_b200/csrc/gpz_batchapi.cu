@@ -1,14 +1,15 @@
-// gpz_batchapi.cu -- C ABI of the batched compress (include/gpz_b200.h,
-// gpz_batch_*): plan creation, graph capture, launch and results.
+// gpz_batchapi.cu -- batched compress / decompress: workspace layout, table
+// building and kernel launches (gpz_batch_host.h), and the plan API of
+// include/gpz_b200.h (gpz_batch_*, gpz_dbatch_*), which captures them in a
+// CUDA graph.
 //
-// Device memory of a batch (one allocation):
-//   [controls: 256 B per snapshot][rel controls: 256 B per snapshot]
-//   [look-back words: one per 8-chunk group of every snapshot][claim counters]
-//     -- zeroed at the start of every launch (a memset node of the graph)
-//   [per class: item descriptors (BItem<T>), group map, rel-block map]
-// Classes are (float, 2D), (float, 3D), (double, 2D), (double, 3D); the graph
-// runs them one after another: rel->abs (when any of its snapshots asks for
-// it), sampling, persistent compress.
+// Classes are (float, 2D), (float, 3D), (double, 2D), (double, 3D); a batch
+// runs them one after another: (compress) rel->abs when any of its snapshots
+// asks for it, sampling, one persistent compress kernel; (decompress) a header
+// check per stream, one persistent decompress kernel.  Two different codec
+// kernels resident on one SM thrash its instruction cache (each is a few
+// hundred KB of unrolled code), which costs far more than overlapping the
+// classes would gain.
 
 #include <algorithm>
 #include <cstring>
@@ -17,25 +18,20 @@
 
 #include "gpz_b200.h"
 #include "gpz_batch.cuh"
+#include "gpz_batch_host.h"
 
 using namespace gpzb;
 
 namespace {
 
 constexpr uint64_t kRelPointsPerBlock = 1u << 16;  // points per rel->abs block of a snapshot
-constexpr uint32_t kRelMaxBlocks = 256;
+constexpr uint64_t kRelMaxBlocks = 256;
 
 inline uint64_t align256(uint64_t v) { return (v + 255u) & ~255ull; }
-
+inline uint64_t chunks_of(uint64_t n) { return (n + kChunk - 1) / kChunk; }
+inline uint64_t groups_of(uint64_t n) { return (chunks_of(n) + kEncWarps - 1) / kEncWarps; }
+inline uint64_t rel_blocks_of(uint64_t n) { return std::min(kRelMaxBlocks, std::max<uint64_t>(1, n / kRelPointsPerBlock)); }
 int class_of(uint32_t bits, uint32_t dim) { return (bits == 64 ? 2 : 0) + (dim == 3 ? 1 : 0); }
-
-struct ClassPlan {
-  std::vector<uint32_t> items;  // batch indices, in work-list order
-  uint64_t groups = 0;          // 8-chunk groups of all its snapshots
-  uint64_t rel_blocks = 0;      // rel->abs blocks (snapshots with GPZ_FLAG_REL_ON_DEVICE)
-  uint64_t table_off = 0, map_off = 0, rmap_off = 0;
-  int grid = 0;
-};
 
 template <typename T>
 void fill_item(BItem<T> &bi, const gpz_batch_item &it, uint8_t *dev, uint64_t ctl_off, uint64_t rctl_off,
@@ -49,7 +45,7 @@ void fill_item(BItem<T> &bi, const gpz_batch_item &it, uint8_t *dev, uint64_t ct
   bi.a.ctl = reinterpret_cast<Control *>(dev + ctl_off);
   bi.a.look = reinterpret_cast<unsigned long long *>(dev + look_off);
   bi.a.n = it.n;
-  bi.a.G = (it.n + kChunk - 1) / kChunk;
+  bi.a.G = chunks_of(it.n);
   bi.a.eb = (T)it.eb;
   bi.a.dim = it.dim;
   auto al = [](const void *p) { return ((uintptr_t)p & 15u) == 0; };
@@ -60,6 +56,21 @@ void fill_item(BItem<T> &bi, const gpz_batch_item &it, uint8_t *dev, uint64_t ct
   bi.rel_mode = it.rel_mode;
   bi.flags = ((it.flags & GPZ_FLAG_SEG_FIXED) ? kBatchSegFixed : 0u) | ((it.flags & GPZ_FLAG_SAFE31) ? kBatchSafe31 : 0u) |
              ((it.flags & GPZ_FLAG_REL_ON_DEVICE) ? kBatchRelDev : 0u);
+}
+
+template <typename T>
+void fill_ditem(DItem<T> &d, const gpz_dbatch_item &it, Control *ctl) {
+  memset(&d, 0, sizeof(d));
+  d.a.s = static_cast<const uint8_t *>(it.d_stream);
+  d.a.bytes = it.stream_bytes;
+  d.a.x = static_cast<T *>(it.d_x);
+  d.a.y = static_cast<T *>(it.d_y);
+  d.a.z = static_cast<T *>(it.dim == 3 ? it.d_z : it.d_y);
+  d.a.cap = it.out_capacity;
+  d.a.ctl = ctl;
+  auto al = [](const void *p) { return ((uintptr_t)p & 15u) == 0; };
+  d.a.vec_ok = al(it.d_x) && al(it.d_y) && (it.dim == 2 || al(it.d_z));
+  d.n = it.n;
 }
 
 // findMinimumValues + convertRelEb for the GPZ_FLAG_REL_ON_DEVICE snapshots
@@ -81,37 +92,275 @@ int num_sms_now() {
   return sms > 0 ? sms : 148;
 }
 
-template <typename T, int DIM>
-int compress_grid(uint64_t groups) {
-  auto k = compress_batch_kernel<T, DIM>;
-  const size_t smem = enc_smem_bytes();
-  if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) return -1;
+// CTAs per SM of a kernel with `smem` dynamic shared memory (the attribute is
+// set once per kernel and process; 0 when the query fails).
+template <typename K>
+int resident_ctas(K kernel, int threads, size_t smem, int &cache) {
+  if (cache) return cache;
+  if (cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) return 0;
   int occ = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k, 32 * kEncWarps, smem) != cudaSuccess || occ < 1) occ = 1;
-  return (int)std::min<uint64_t>(groups, (uint64_t)num_sms_now() * occ);
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kernel, threads, smem) != cudaSuccess || occ < 1) occ = 1;
+  cache = occ;
+  return occ;
 }
 
 template <typename T, int DIM>
-void enqueue_class(const ClassPlan &cp, uint8_t *dev, uint64_t claim_off, cudaStream_t st) {
+int compress_grid(uint64_t groups) {
+  static int occ = 0;
+  const int o = resident_ctas(compress_batch_kernel<T, DIM>, 32 * kEncWarps, enc_smem_bytes(), occ);
+  return o ? (int)std::min<uint64_t>(groups, (uint64_t)num_sms_now() * o) : -1;
+}
+
+template <typename T, int DIM>
+int dec_grid(uint64_t chunks) {
+  static int occ = 0;
+  constexpr int W = DecCfg<T>::warps;
+  const int o = resident_ctas(decompress_batch_kernel<T, DIM>, 32 * W, dec_smem_bytes<T>(), occ);
+  return o ? (int)std::min<uint64_t>((chunks + W - 1) / W, (uint64_t)num_sms_now() * o) : -1;
+}
+
+template <typename T, int DIM>
+void enqueue_class(const gpzb_host::ClassPlan &cp, uint8_t *dev, uint64_t claim_off, cudaStream_t st) {
   BItem<T> *tab = reinterpret_cast<BItem<T> *>(dev + cp.table_off);
-  const unsigned long long *map = reinterpret_cast<const unsigned long long *>(dev + cp.map_off);
   if (cp.rel_blocks)
     batch_rel_mapped_kernel<T><<<(unsigned)cp.rel_blocks, 256, 0, st>>>(
         tab, reinterpret_cast<const unsigned long long *>(dev + cp.rmap_off));
   batch_sample_kernel<T><<<dim3(128, (unsigned)cp.items.size()), 256, 0, st>>>(tab);
   compress_batch_kernel<T, DIM><<<cp.grid, 32 * kEncWarps, enc_smem_bytes(), st>>>(
-      tab, map, cp.groups, reinterpret_cast<unsigned long long *>(dev + claim_off));
+      tab, reinterpret_cast<const unsigned long long *>(dev + cp.map_off), cp.work,
+      reinterpret_cast<unsigned long long *>(dev + claim_off));
+}
+
+template <typename T, int DIM>
+void enqueue_dclass(const gpzb_host::ClassPlan &cp, uint8_t *dev, cudaStream_t st) {
+  DItem<T> *tab = reinterpret_cast<DItem<T> *>(dev + cp.table_off);
+  const uint32_t K = (uint32_t)cp.items.size();
+  dbatch_header_kernel<T, DIM><<<(K + 127) / 128, 128, 0, st>>>(tab, K);
+  decompress_batch_kernel<T, DIM><<<cp.grid, 32 * DecCfg<T>::warps, dec_smem_bytes<T>(), st>>>(
+      tab, reinterpret_cast<const unsigned long long *>(dev + cp.map_off), cp.work);
+}
+
+}  // namespace
+
+// ===========================================================================
+// Workspace layout, tables, launches.
+// ===========================================================================
+namespace gpzb_host {
+
+bool compress_item_ok(const gpz_batch_item &it) {
+  const uint64_t hdr = it.float_bits == 64 ? 32 : 24, meta = it.float_bits == 64 ? 64 : 36;
+  return (it.float_bits == 32 || it.float_bits == 64) && (it.dim == 2 || it.dim == 3) && it.n >= 1 && it.d_x &&
+         it.d_y && (it.dim == 2 || it.d_z) && it.d_out && it.out_capacity >= hdr + chunks_of(it.n) * (8 + meta) &&
+         !((it.flags & GPZ_FLAG_SEG_FIXED) && it.seg_size == 0) &&
+         (it.flags & ~(GPZ_FLAG_SAFE31 | GPZ_FLAG_SEG_FIXED | GPZ_FLAG_REL_ON_DEVICE)) == 0;
+}
+
+bool decompress_item_ok(const gpz_dbatch_item &it) {
+  return (it.float_bits == 32 || it.float_bits == 64) && (it.dim == 2 || it.dim == 3) && it.n >= 1 && it.d_stream &&
+         ((uintptr_t)it.d_stream & 7u) == 0 && it.d_x && it.d_y && (it.dim == 2 || it.d_z) && it.out_capacity >= it.n;
+}
+
+bool compress_layout(const gpz_batch_item *items, uint32_t count, Layout &L) {
+  L = Layout();
+  L.count = count;
+  L.look_off.resize(count);
+  uint64_t off = 2ull * count * kCtlBytes;
+  for (uint32_t i = 0; i < count; ++i) {
+    L.look_off[i] = off;
+    off += 8 * groups_of(items[i].n);
+    ClassPlan &cp = L.cls[class_of(items[i].float_bits, items[i].dim)];
+    cp.items.push_back(i);
+    cp.work += groups_of(items[i].n);
+    if (items[i].flags & GPZ_FLAG_REL_ON_DEVICE) cp.rel_blocks += rel_blocks_of(items[i].n);
+  }
+  L.claim_off = align256(off);
+  L.zero_bytes = L.claim_off + 4 * 8;
+  off = align256(L.zero_bytes);
+  for (int c = 0; c < 4; ++c) {
+    ClassPlan &cp = L.cls[c];
+    if (cp.items.empty()) continue;
+    cp.table_off = off;
+    off = align256(off + (c < 2 ? sizeof(BItem<float>) : sizeof(BItem<double>)) * cp.items.size());
+    cp.map_off = off;
+    off = align256(off + 8 * cp.work);
+    cp.rmap_off = off;
+    off = align256(off + 8 * cp.rel_blocks);
+    switch (c) {
+      case 0: cp.grid = compress_grid<float, 2>(cp.work); break;
+      case 1: cp.grid = compress_grid<float, 3>(cp.work); break;
+      case 2: cp.grid = compress_grid<double, 2>(cp.work); break;
+      default: cp.grid = compress_grid<double, 3>(cp.work); break;
+    }
+    if (cp.grid < 1) return false;
+  }
+  L.bytes = off;
+  return true;
+}
+
+bool decompress_layout(const gpz_dbatch_item *items, uint32_t count, Layout &L) {
+  L = Layout();
+  L.count = count;
+  for (uint32_t i = 0; i < count; ++i) {
+    ClassPlan &cp = L.cls[class_of(items[i].float_bits, items[i].dim)];
+    cp.items.push_back(i);
+    cp.work += chunks_of(items[i].n);
+  }
+  L.zero_bytes = (uint64_t)count * kCtlBytes;
+  uint64_t off = align256(L.zero_bytes);
+  for (int c = 0; c < 4; ++c) {
+    ClassPlan &cp = L.cls[c];
+    if (cp.items.empty()) continue;
+    cp.table_off = off;
+    off = align256(off + (c < 2 ? sizeof(DItem<float>) : sizeof(DItem<double>)) * cp.items.size());
+    cp.map_off = off;
+    off = align256(off + 8 * cp.work);
+    switch (c) {
+      case 0: cp.grid = dec_grid<float, 2>(cp.work); break;
+      case 1: cp.grid = dec_grid<float, 3>(cp.work); break;
+      case 2: cp.grid = dec_grid<double, 2>(cp.work); break;
+      default: cp.grid = dec_grid<double, 3>(cp.work); break;
+    }
+    if (cp.grid < 1) return false;
+  }
+  L.bytes = off;
+  return true;
+}
+
+void compress_tables(const gpz_batch_item *items, const Layout &L, uint8_t *dev, uint8_t *image) {
+  auto H = [&](uint64_t dev_off) { return image + (dev_off - L.zero_bytes); };
+  for (int c = 0; c < 4; ++c) {
+    const ClassPlan &cp = L.cls[c];
+    if (cp.items.empty()) continue;
+    uint64_t g = 0, rb = 0;
+    unsigned long long *map = reinterpret_cast<unsigned long long *>(H(cp.map_off));
+    unsigned long long *rmap = reinterpret_cast<unsigned long long *>(H(cp.rmap_off));
+    for (size_t k = 0; k < cp.items.size(); ++k) {
+      const uint32_t i = cp.items[k];
+      const gpz_batch_item &it = items[i];
+      if (c < 2) fill_item<float>(reinterpret_cast<BItem<float> *>(H(cp.table_off))[k], it, dev, ctl_off(i),
+                                  ctl_off(L.count + i), L.look_off[i]);
+      else fill_item<double>(reinterpret_cast<BItem<double> *>(H(cp.table_off))[k], it, dev, ctl_off(i),
+                             ctl_off(L.count + i), L.look_off[i]);
+      const uint64_t groups = groups_of(it.n);
+      for (uint64_t q = 0; q < groups; ++q) map[g++] = ((unsigned long long)k << kBatchLocalBits) | q;
+      if (it.flags & GPZ_FLAG_REL_ON_DEVICE) {
+        const uint64_t nb = rel_blocks_of(it.n);
+        for (uint64_t q = 0; q < nb; ++q) rmap[rb++] = ((unsigned long long)k << 40) | (nb << 20) | q;
+      }
+    }
+  }
+}
+
+void decompress_tables(const gpz_dbatch_item *items, const Layout &L, uint8_t *dev, uint8_t *image) {
+  auto H = [&](uint64_t dev_off) { return image + (dev_off - L.zero_bytes); };
+  for (int c = 0; c < 4; ++c) {
+    const ClassPlan &cp = L.cls[c];
+    if (cp.items.empty()) continue;
+    uint64_t q = 0;
+    unsigned long long *map = reinterpret_cast<unsigned long long *>(H(cp.map_off));
+    for (size_t k = 0; k < cp.items.size(); ++k) {
+      const uint32_t i = cp.items[k];
+      Control *ctl = reinterpret_cast<Control *>(dev + ctl_off(i));
+      if (c < 2) fill_ditem<float>(reinterpret_cast<DItem<float> *>(H(cp.table_off))[k], items[i], ctl);
+      else fill_ditem<double>(reinterpret_cast<DItem<double> *>(H(cp.table_off))[k], items[i], ctl);
+      const uint64_t G = chunks_of(items[i].n);
+      for (uint64_t ch = 0; ch < G; ++ch) map[q++] = ((unsigned long long)k << kBatchLocalBits) | ch;
+    }
+  }
+}
+
+void compress_enqueue(const Layout &L, uint8_t *dev, cudaStream_t st) {
+  cudaMemsetAsync(dev, 0, L.zero_bytes, st);
+  for (int c = 0; c < 4; ++c) {
+    if (L.cls[c].items.empty()) continue;
+    const uint64_t claim = L.claim_off + 8ull * c;
+    switch (c) {
+      case 0: enqueue_class<float, 2>(L.cls[c], dev, claim, st); break;
+      case 1: enqueue_class<float, 3>(L.cls[c], dev, claim, st); break;
+      case 2: enqueue_class<double, 2>(L.cls[c], dev, claim, st); break;
+      default: enqueue_class<double, 3>(L.cls[c], dev, claim, st); break;
+    }
+  }
+}
+
+void decompress_enqueue(const Layout &L, uint8_t *dev, cudaStream_t st) {
+  cudaMemsetAsync(dev, 0, L.zero_bytes, st);
+  for (int c = 0; c < 4; ++c) {
+    if (L.cls[c].items.empty()) continue;
+    switch (c) {
+      case 0: enqueue_dclass<float, 2>(L.cls[c], dev, st); break;
+      case 1: enqueue_dclass<float, 3>(L.cls[c], dev, st); break;
+      case 2: enqueue_dclass<double, 2>(L.cls[c], dev, st); break;
+      default: enqueue_dclass<double, 3>(L.cls[c], dev, st); break;
+    }
+  }
+}
+
+}  // namespace gpzb_host
+
+// ===========================================================================
+// Plans: the workspace allocated once, the launches captured in a graph.
+// ===========================================================================
+namespace {
+
+struct Plan {
+  uint32_t count = 0;
+  uint8_t *mem = nullptr;
+  uint64_t bytes = 0;
+  cudaGraphExec_t exec = nullptr;
+  ~Plan() {
+    if (exec) cudaGraphExecDestroy(exec);
+    if (mem) cudaFree(mem);
+  }
+};
+
+// Allocates the workspace, uploads the table image built by `tables` and
+// captures `enqueue` into the plan's graph.
+template <typename Tables, typename Enq>
+int make_plan(Plan &p, const gpzb_host::Layout &L, Tables tables, Enq enqueue) {
+  p.count = L.count;
+  p.bytes = L.bytes;
+  if (cudaMalloc(&p.mem, p.bytes) != cudaSuccess) {
+    p.mem = nullptr;
+    return GPZ_ECUDA;
+  }
+  std::vector<uint8_t> image(L.bytes - L.zero_bytes);
+  tables(p.mem, image.data());
+  if (cudaMemcpy(p.mem + L.zero_bytes, image.data(), image.size(), cudaMemcpyHostToDevice) != cudaSuccess)
+    return GPZ_ECUDA;
+  cudaStream_t s0 = nullptr;
+  cudaGraph_t graph = nullptr;
+  bool ok = cudaStreamCreateWithFlags(&s0, cudaStreamNonBlocking) == cudaSuccess &&
+            cudaStreamBeginCapture(s0, cudaStreamCaptureModeThreadLocal) == cudaSuccess;
+  if (ok) {
+    enqueue(p.mem, s0);
+    ok = cudaStreamEndCapture(s0, &graph) == cudaSuccess && graph;
+  }
+  if (ok) ok = cudaGraphInstantiate(&p.exec, graph, 0) == cudaSuccess;
+  if (graph) cudaGraphDestroy(graph);
+  if (s0) cudaStreamDestroy(s0);
+  if (!ok) cudaGetLastError();
+  return ok ? GPZ_OK : GPZ_ECUDA;
+}
+
+int read_controls(const uint8_t *dev, uint32_t blocks, std::vector<Control> &h, cudaStream_t st) {
+  h.resize(blocks);
+  for (uint32_t i = 0; i < blocks; ++i)
+    if (cudaMemcpyAsync(&h[i], dev + gpzb_host::ctl_off(i), sizeof(Control), cudaMemcpyDeviceToHost, st) !=
+        cudaSuccess)
+      return GPZ_ECUDA;
+  return cudaStreamSynchronize(st) == cudaSuccess ? GPZ_OK : GPZ_ECUDA;
 }
 
 }  // namespace
 
 struct gpz_batch {
-  int device = 0;
-  uint32_t count = 0;
-  uint8_t *mem = nullptr;
-  uint64_t bytes = 0, zero_bytes = 0;
+  Plan plan;
   std::vector<gpz_batch_item> items;
-  cudaGraphExec_t exec = nullptr;
+};
+
+struct gpz_dbatch {
+  Plan plan;
 };
 
 extern "C" {
@@ -119,150 +368,39 @@ extern "C" {
 int gpz_batch_create(const gpz_batch_item *items, uint32_t count, gpz_batch **batch, uint32_t *bad_item) {
   if (!batch || !items || count == 0) return GPZ_EINVAL;
   *batch = nullptr;
-  for (uint32_t i = 0; i < count; ++i) {
-    const gpz_batch_item &it = items[i];
-    const uint64_t G = (it.n + kChunk - 1) / kChunk;
-    const uint64_t hdr = it.float_bits == 64 ? 32 : 24, meta = it.float_bits == 64 ? 64 : 36;
-    const bool ok = (it.float_bits == 32 || it.float_bits == 64) && (it.dim == 2 || it.dim == 3) && it.n >= 1 &&
-                    it.d_x && it.d_y && (it.dim == 2 || it.d_z) && it.d_out &&
-                    it.out_capacity >= hdr + G * (8 + meta) && !((it.flags & GPZ_FLAG_SEG_FIXED) && it.seg_size == 0) &&
-                    (it.flags & ~(GPZ_FLAG_SAFE31 | GPZ_FLAG_SEG_FIXED | GPZ_FLAG_REL_ON_DEVICE)) == 0;
-    if (!ok) {
+  for (uint32_t i = 0; i < count; ++i)
+    if (!gpzb_host::compress_item_ok(items[i])) {
       if (bad_item) *bad_item = i;
       return GPZ_EINVAL;
     }
-  }
+  gpzb_host::Layout L;
+  if (!gpzb_host::compress_layout(items, count, L)) return GPZ_ECUDA;
   gpz_batch *b = new (std::nothrow) gpz_batch;
   if (!b) return GPZ_ECUDA;
-  b->count = count;
   b->items.assign(items, items + count);
-  cudaGetDevice(&b->device);
-
-  // ---- layout
-  ClassPlan cls[4];
-  std::vector<uint64_t> look_off(count);
-  uint64_t off = 2ull * count * kCtlBytes;
-  for (uint32_t i = 0; i < count; ++i) {
-    const uint64_t G = (items[i].n + kChunk - 1) / kChunk, groups = (G + kEncWarps - 1) / kEncWarps;
-    look_off[i] = off;
-    off += 8 * groups;
-    ClassPlan &cp = cls[class_of(items[i].float_bits, items[i].dim)];
-    cp.items.push_back(i);
-    cp.groups += groups;
-    if (items[i].flags & GPZ_FLAG_REL_ON_DEVICE)
-      cp.rel_blocks += std::min<uint64_t>(kRelMaxBlocks, std::max<uint64_t>(1, items[i].n / kRelPointsPerBlock));
-  }
-  const uint64_t claim_off = align256(off);
-  b->zero_bytes = claim_off + 4 * 8;
-  off = align256(b->zero_bytes);
-  for (int c = 0; c < 4; ++c) {
-    if (cls[c].items.empty()) continue;
-    const uint64_t isz = c < 2 ? sizeof(BItem<float>) : sizeof(BItem<double>);
-    cls[c].table_off = off;
-    off = align256(off + isz * cls[c].items.size());
-    cls[c].map_off = off;
-    off = align256(off + 8 * cls[c].groups);
-    cls[c].rmap_off = off;
-    off = align256(off + 8 * cls[c].rel_blocks);
-  }
-  b->bytes = off;
-  if (cudaMalloc(&b->mem, b->bytes) != cudaSuccess) {
+  const int rc = make_plan(
+      b->plan, L, [&](uint8_t *dev, uint8_t *image) { gpzb_host::compress_tables(items, L, dev, image); },
+      [&](uint8_t *dev, cudaStream_t s) { gpzb_host::compress_enqueue(L, dev, s); });
+  if (rc != GPZ_OK) {
     delete b;
-    return GPZ_ECUDA;
-  }
-
-  // ---- descriptors and maps (host-built, uploaded once)
-  std::vector<uint8_t> host(b->bytes - b->zero_bytes);
-  auto H = [&](uint64_t dev_off) { return host.data() + (dev_off - b->zero_bytes); };
-  for (int c = 0; c < 4; ++c) {
-    ClassPlan &cp = cls[c];
-    if (cp.items.empty()) continue;
-    uint64_t g = 0, rb = 0;
-    for (size_t k = 0; k < cp.items.size(); ++k) {
-      const uint32_t i = cp.items[k];
-      const gpz_batch_item &it = items[i];
-      if (c < 2) fill_item<float>(reinterpret_cast<BItem<float> *>(H(cp.table_off))[k], it, b->mem,
-                                  (uint64_t)i * kCtlBytes, (uint64_t)(count + i) * kCtlBytes, look_off[i]);
-      else fill_item<double>(reinterpret_cast<BItem<double> *>(H(cp.table_off))[k], it, b->mem,
-                             (uint64_t)i * kCtlBytes, (uint64_t)(count + i) * kCtlBytes, look_off[i]);
-      const uint64_t G = (it.n + kChunk - 1) / kChunk, groups = (G + kEncWarps - 1) / kEncWarps;
-      unsigned long long *map = reinterpret_cast<unsigned long long *>(H(cp.map_off));
-      for (uint64_t q = 0; q < groups; ++q) map[g++] = ((unsigned long long)k << kBatchLocalBits) | q;
-      if (it.flags & GPZ_FLAG_REL_ON_DEVICE) {
-        const uint64_t nb = std::min<uint64_t>(kRelMaxBlocks, std::max<uint64_t>(1, it.n / kRelPointsPerBlock));
-        unsigned long long *rmap = reinterpret_cast<unsigned long long *>(H(cp.rmap_off));
-        for (uint64_t q = 0; q < nb; ++q) rmap[rb++] = ((unsigned long long)k << 40) | (nb << 20) | q;
-      }
-    }
-    switch (c) {
-      case 0: cp.grid = compress_grid<float, 2>(cp.groups); break;
-      case 1: cp.grid = compress_grid<float, 3>(cp.groups); break;
-      case 2: cp.grid = compress_grid<double, 2>(cp.groups); break;
-      default: cp.grid = compress_grid<double, 3>(cp.groups); break;
-    }
-    if (cp.grid < 1) {
-      cudaFree(b->mem);
-      delete b;
-      return GPZ_ECUDA;
-    }
-  }
-  if (cudaMemcpy(b->mem + b->zero_bytes, host.data(), host.size(), cudaMemcpyHostToDevice) != cudaSuccess) {
-    cudaFree(b->mem);
-    delete b;
-    return GPZ_ECUDA;
-  }
-
-  // ---- graph: memset, then one branch per class
-  cudaStream_t s0 = nullptr;
-  cudaGraph_t graph = nullptr;
-  bool okc = cudaStreamCreateWithFlags(&s0, cudaStreamNonBlocking) == cudaSuccess;
-  if (okc) okc = cudaStreamBeginCapture(s0, cudaStreamCaptureModeThreadLocal) == cudaSuccess;
-  if (okc) {
-    // The classes run one after another: two different compress kernels
-    // resident on one SM thrash its instruction cache (each is a few hundred
-    // KB of unrolled code), which costs far more than the overlap gains.
-    cudaMemsetAsync(b->mem, 0, b->zero_bytes, s0);
-    for (int c = 0; c < 4; ++c) {
-      if (cls[c].items.empty()) continue;
-      const uint64_t claim = claim_off + 8ull * c;
-      switch (c) {
-        case 0: enqueue_class<float, 2>(cls[c], b->mem, claim, s0); break;
-        case 1: enqueue_class<float, 3>(cls[c], b->mem, claim, s0); break;
-        case 2: enqueue_class<double, 2>(cls[c], b->mem, claim, s0); break;
-        default: enqueue_class<double, 3>(cls[c], b->mem, claim, s0); break;
-      }
-    }
-    okc = cudaStreamEndCapture(s0, &graph) == cudaSuccess && graph;
-  }
-  if (okc) okc = cudaGraphInstantiate(&b->exec, graph, 0) == cudaSuccess;
-  if (graph) cudaGraphDestroy(graph);
-  if (s0) cudaStreamDestroy(s0);
-  if (!okc) {
-    cudaGetLastError();
-    cudaFree(b->mem);
-    delete b;
-    return GPZ_ECUDA;
+    return rc;
   }
   *batch = b;
   return GPZ_OK;
 }
 
 int gpz_batch_launch(gpz_batch *b, void *stream) {
-  if (!b || !b->exec) return GPZ_EINVAL;
-  return cudaGraphLaunch(b->exec, static_cast<cudaStream_t>(stream)) == cudaSuccess ? GPZ_OK : GPZ_ECUDA;
+  if (!b || !b->plan.exec) return GPZ_EINVAL;
+  return cudaGraphLaunch(b->plan.exec, static_cast<cudaStream_t>(stream)) == cudaSuccess ? GPZ_OK : GPZ_ECUDA;
 }
 
 int gpz_batch_results(gpz_batch *b, gpz_result *results, double *h_eb, void *stream) {
   if (!b || !results) return GPZ_EINVAL;
-  cudaStream_t st = static_cast<cudaStream_t>(stream);
-  std::vector<Control> h(2ull * b->count);
-  static_assert(sizeof(Control) <= kCtlBytes, "control block");
-  for (uint32_t i = 0; i < 2 * b->count; ++i)
-    if (cudaMemcpyAsync(&h[i], b->mem + (uint64_t)i * kCtlBytes, sizeof(Control), cudaMemcpyDeviceToHost, st) !=
-        cudaSuccess)
-      return GPZ_ECUDA;
-  if (cudaStreamSynchronize(st) != cudaSuccess) return GPZ_ECUDA;
-  for (uint32_t i = 0; i < b->count; ++i) {
+  const uint32_t n = b->plan.count;
+  std::vector<Control> h;
+  const int rc = read_controls(b->plan.mem, 2 * n, h, static_cast<cudaStream_t>(stream));
+  if (rc != GPZ_OK) return rc;
+  for (uint32_t i = 0; i < n; ++i) {
     const Control &c = h[i];
     results[i].stream_bytes = c.stream_bytes;
     results[i].seg_size = c.seg;
@@ -271,196 +409,55 @@ int gpz_batch_results(gpz_batch *b, gpz_result *results, double *h_eb, void *str
     results[i].id_overflow = c.id_overflow;
     if (h_eb) {
       const gpz_batch_item &it = b->items[i];
-      if (it.flags & GPZ_FLAG_REL_ON_DEVICE) h_eb[i] = h[b->count + i].out_eb;
+      if (it.flags & GPZ_FLAG_REL_ON_DEVICE) h_eb[i] = h[n + i].out_eb;
       else h_eb[i] = it.float_bits == 32 ? (double)(float)it.eb : it.eb;
     }
   }
   return GPZ_OK;
 }
 
-uint64_t gpz_batch_device_bytes(const gpz_batch *b) { return b ? b->bytes : 0; }
+uint64_t gpz_batch_device_bytes(const gpz_batch *b) { return b ? b->plan.bytes : 0; }
 
 int gpz_batch_destroy(gpz_batch *b) {
   if (!b) return GPZ_EINVAL;
-  if (b->exec) cudaGraphExecDestroy(b->exec);
-  if (b->mem) cudaFree(b->mem);
   delete b;
   return GPZ_OK;
 }
 
-}  // extern "C"
-
-// ===========================================================================
-// Batched decompress.
-// ===========================================================================
-namespace {
-
-template <typename T, int DIM>
-int dec_grid(uint64_t chunks) {
-  auto k = decompress_batch_kernel<T, DIM>;
-  constexpr size_t smem = dec_smem_bytes<T>();
-  constexpr int W = DecCfg<T>::warps;
-  if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) return -1;
-  int occ = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k, 32 * W, smem) != cudaSuccess || occ < 1) occ = 1;
-  return (int)std::min<uint64_t>((chunks + W - 1) / W, (uint64_t)num_sms_now() * occ);
-}
-
-struct DClass {
-  std::vector<uint32_t> items;
-  uint64_t chunks = 0, table_off = 0, map_off = 0;
-  int grid = 0;
-};
-
-template <typename T, int DIM>
-void enqueue_dclass(const DClass &cp, uint8_t *dev, cudaStream_t st) {
-  DItem<T> *tab = reinterpret_cast<DItem<T> *>(dev + cp.table_off);
-  const uint32_t K = (uint32_t)cp.items.size();
-  dbatch_header_kernel<T, DIM><<<(K + 127) / 128, 128, 0, st>>>(tab, K);
-  decompress_batch_kernel<T, DIM><<<cp.grid, 32 * DecCfg<T>::warps, dec_smem_bytes<T>(), st>>>(
-      tab, reinterpret_cast<const unsigned long long *>(dev + cp.map_off), cp.chunks);
-}
-
-template <typename T>
-void fill_ditem(DItem<T> &d, const gpz_dbatch_item &it, Control *ctl) {
-  memset(&d, 0, sizeof(d));
-  d.a.s = static_cast<const uint8_t *>(it.d_stream);
-  d.a.bytes = it.stream_bytes;
-  d.a.x = static_cast<T *>(it.d_x);
-  d.a.y = static_cast<T *>(it.d_y);
-  d.a.z = static_cast<T *>(it.dim == 3 ? it.d_z : it.d_y);
-  d.a.cap = it.out_capacity;
-  d.a.ctl = ctl;
-  auto al = [](const void *p) { return ((uintptr_t)p & 15u) == 0; };
-  d.a.vec_ok = al(it.d_x) && al(it.d_y) && (it.dim == 2 || al(it.d_z));
-  d.n = it.n;
-}
-
-}  // namespace
-
-struct gpz_dbatch {
-  uint32_t count = 0;
-  uint8_t *mem = nullptr;
-  uint64_t bytes = 0, zero_bytes = 0;
-  cudaGraphExec_t exec = nullptr;
-};
-
-extern "C" {
-
 int gpz_dbatch_create(const gpz_dbatch_item *items, uint32_t count, gpz_dbatch **batch, uint32_t *bad_item) {
   if (!batch || !items || count == 0) return GPZ_EINVAL;
   *batch = nullptr;
-  for (uint32_t i = 0; i < count; ++i) {
-    const gpz_dbatch_item &it = items[i];
-    const bool ok = (it.float_bits == 32 || it.float_bits == 64) && (it.dim == 2 || it.dim == 3) && it.n >= 1 &&
-                    it.d_stream && ((uintptr_t)it.d_stream & 7u) == 0 && it.d_x && it.d_y &&
-                    (it.dim == 2 || it.d_z) && it.out_capacity >= it.n;
-    if (!ok) {
+  for (uint32_t i = 0; i < count; ++i)
+    if (!gpzb_host::decompress_item_ok(items[i])) {
       if (bad_item) *bad_item = i;
       return GPZ_EINVAL;
     }
-  }
+  gpzb_host::Layout L;
+  if (!gpzb_host::decompress_layout(items, count, L)) return GPZ_ECUDA;
   gpz_dbatch *b = new (std::nothrow) gpz_dbatch;
   if (!b) return GPZ_ECUDA;
-  b->count = count;
-  DClass cls[4];
-  for (uint32_t i = 0; i < count; ++i) {
-    DClass &cp = cls[class_of(items[i].float_bits, items[i].dim)];
-    cp.items.push_back(i);
-    cp.chunks += (items[i].n + kChunk - 1) / kChunk;
-  }
-  b->zero_bytes = (uint64_t)count * kCtlBytes;
-  uint64_t off = align256(b->zero_bytes);
-  for (int c = 0; c < 4; ++c) {
-    if (cls[c].items.empty()) continue;
-    const uint64_t isz = c < 2 ? sizeof(DItem<float>) : sizeof(DItem<double>);
-    cls[c].table_off = off;
-    off = align256(off + isz * cls[c].items.size());
-    cls[c].map_off = off;
-    off = align256(off + 8 * cls[c].chunks);
-  }
-  b->bytes = off;
-  if (cudaMalloc(&b->mem, b->bytes) != cudaSuccess) {
+  const int rc = make_plan(
+      b->plan, L, [&](uint8_t *dev, uint8_t *image) { gpzb_host::decompress_tables(items, L, dev, image); },
+      [&](uint8_t *dev, cudaStream_t s) { gpzb_host::decompress_enqueue(L, dev, s); });
+  if (rc != GPZ_OK) {
     delete b;
-    return GPZ_ECUDA;
-  }
-  std::vector<uint8_t> host(b->bytes - b->zero_bytes);
-  auto H = [&](uint64_t dev_off) { return host.data() + (dev_off - b->zero_bytes); };
-  for (int c = 0; c < 4; ++c) {
-    DClass &cp = cls[c];
-    if (cp.items.empty()) continue;
-    uint64_t q = 0;
-    for (size_t k = 0; k < cp.items.size(); ++k) {
-      const uint32_t i = cp.items[k];
-      Control *ctl = reinterpret_cast<Control *>(b->mem + (uint64_t)i * kCtlBytes);
-      if (c < 2) fill_ditem<float>(reinterpret_cast<DItem<float> *>(H(cp.table_off))[k], items[i], ctl);
-      else fill_ditem<double>(reinterpret_cast<DItem<double> *>(H(cp.table_off))[k], items[i], ctl);
-      const uint64_t G = (items[i].n + kChunk - 1) / kChunk;
-      unsigned long long *map = reinterpret_cast<unsigned long long *>(H(cp.map_off));
-      for (uint64_t ch = 0; ch < G; ++ch) map[q++] = ((unsigned long long)k << kBatchLocalBits) | ch;
-    }
-    switch (c) {
-      case 0: cp.grid = dec_grid<float, 2>(cp.chunks); break;
-      case 1: cp.grid = dec_grid<float, 3>(cp.chunks); break;
-      case 2: cp.grid = dec_grid<double, 2>(cp.chunks); break;
-      default: cp.grid = dec_grid<double, 3>(cp.chunks); break;
-    }
-    if (cp.grid < 1) {
-      cudaFree(b->mem);
-      delete b;
-      return GPZ_ECUDA;
-    }
-  }
-  if (cudaMemcpy(b->mem + b->zero_bytes, host.data(), host.size(), cudaMemcpyHostToDevice) != cudaSuccess) {
-    cudaFree(b->mem);
-    delete b;
-    return GPZ_ECUDA;
-  }
-  cudaStream_t s0 = nullptr;
-  cudaGraph_t graph = nullptr;
-  bool okc = cudaStreamCreateWithFlags(&s0, cudaStreamNonBlocking) == cudaSuccess;
-  if (okc) okc = cudaStreamBeginCapture(s0, cudaStreamCaptureModeThreadLocal) == cudaSuccess;
-  if (okc) {
-    cudaMemsetAsync(b->mem, 0, b->zero_bytes, s0);
-    for (int c = 0; c < 4; ++c) {  // one class after another, as in the compress graph
-      if (cls[c].items.empty()) continue;
-      switch (c) {
-        case 0: enqueue_dclass<float, 2>(cls[c], b->mem, s0); break;
-        case 1: enqueue_dclass<float, 3>(cls[c], b->mem, s0); break;
-        case 2: enqueue_dclass<double, 2>(cls[c], b->mem, s0); break;
-        default: enqueue_dclass<double, 3>(cls[c], b->mem, s0); break;
-      }
-    }
-    okc = cudaStreamEndCapture(s0, &graph) == cudaSuccess && graph;
-  }
-  if (okc) okc = cudaGraphInstantiate(&b->exec, graph, 0) == cudaSuccess;
-  if (graph) cudaGraphDestroy(graph);
-  if (s0) cudaStreamDestroy(s0);
-  if (!okc) {
-    cudaGetLastError();
-    cudaFree(b->mem);
-    delete b;
-    return GPZ_ECUDA;
+    return rc;
   }
   *batch = b;
   return GPZ_OK;
 }
 
 int gpz_dbatch_launch(gpz_dbatch *b, void *stream) {
-  if (!b || !b->exec) return GPZ_EINVAL;
-  return cudaGraphLaunch(b->exec, static_cast<cudaStream_t>(stream)) == cudaSuccess ? GPZ_OK : GPZ_ECUDA;
+  if (!b || !b->plan.exec) return GPZ_EINVAL;
+  return cudaGraphLaunch(b->plan.exec, static_cast<cudaStream_t>(stream)) == cudaSuccess ? GPZ_OK : GPZ_ECUDA;
 }
 
 int gpz_dbatch_results(gpz_dbatch *b, gpz_result *results, void *stream) {
   if (!b || !results) return GPZ_EINVAL;
-  cudaStream_t st = static_cast<cudaStream_t>(stream);
-  std::vector<Control> h(b->count);
-  for (uint32_t i = 0; i < b->count; ++i)
-    if (cudaMemcpyAsync(&h[i], b->mem + (uint64_t)i * kCtlBytes, sizeof(Control), cudaMemcpyDeviceToHost, st) !=
-        cudaSuccess)
-      return GPZ_ECUDA;
-  if (cudaStreamSynchronize(st) != cudaSuccess) return GPZ_ECUDA;
-  for (uint32_t i = 0; i < b->count; ++i) {
+  std::vector<Control> h;
+  const int rc = read_controls(b->plan.mem, b->plan.count, h, static_cast<cudaStream_t>(stream));
+  if (rc != GPZ_OK) return rc;
+  for (uint32_t i = 0; i < b->plan.count; ++i) {
     memset(&results[i], 0, sizeof(gpz_result));
     results[i].status = h[i].status;
   }
@@ -469,8 +466,6 @@ int gpz_dbatch_results(gpz_dbatch *b, gpz_result *results, void *stream) {
 
 int gpz_dbatch_destroy(gpz_dbatch *b) {
   if (!b) return GPZ_EINVAL;
-  if (b->exec) cudaGraphExecDestroy(b->exec);
-  if (b->mem) cudaFree(b->mem);
   delete b;
   return GPZ_OK;
 }

@@ -304,6 +304,80 @@ int gpz_dbatch_launch(gpz_dbatch *batch, void *stream);
 int gpz_dbatch_results(gpz_dbatch *batch, gpz_result *results, void *stream);
 int gpz_dbatch_destroy(gpz_dbatch *batch);
 
+/* ---- request server --------------------------------------------------------------
+ * No counterpart in the reference (a command line tool: one file, one call).
+ * A server admits compress / decompress requests as they arrive and runs them
+ * in batches on several CUDA streams (continuous batching): whenever a stream
+ * is free, every queued request whose output fits in the device-memory budget
+ * joins the next batch, so requests that arrive while others run are started
+ * as soon as a stream and memory free up, and their work overlaps on the GPU.
+ * All device memory -- request outputs and batch workspaces -- comes from one
+ * arena of hbm_budget bytes allocated at creation; serving allocates nothing.
+ * Outputs stay in the arena (device resident) until the caller releases them.
+ * Each request's output equals the single-call API's (gpz_compress with the
+ * same parameters, gpz_decompress). */
+#define GPZ_OP_COMPRESS 1u
+#define GPZ_OP_DECOMPRESS 2u
+
+typedef struct gpz_server_config {
+  uint64_t hbm_budget;      /* bytes of device memory for outputs and workspaces */
+  uint32_t streams;         /* batches in flight at once, >= 1 */
+  uint32_t max_batch;       /* requests per batch, >= 1 */
+  uint64_t workspace_bytes; /* per stream: batch descriptors and control blocks (0: 64 MiB) */
+} gpz_server_config;
+
+typedef struct gpz_request {
+  uint32_t op;              /* GPZ_OP_COMPRESS or GPZ_OP_DECOMPRESS */
+  uint32_t float_bits;      /* compress: the input's; decompress: from the stream header */
+  uint32_t dim;
+  uint32_t flags;           /* compress: GPZ_FLAG_SAFE31 | GPZ_FLAG_SEG_FIXED | GPZ_FLAG_REL_ON_DEVICE */
+  uint64_t n;               /* points (decompress: from the stream header) */
+  const void *d_x;          /* compress input; must stay valid until the request completes */
+  const void *d_y;
+  const void *d_z;
+  const void *d_stream;     /* decompress input; must stay valid until the request completes */
+  uint64_t stream_bytes;
+  double eb;                /* as in gpz_batch_item */
+  double rel_eb;
+  int32_t rel_mode;
+  uint32_t seg_size;
+} gpz_request;
+
+typedef struct gpz_completion {
+  int32_t status;           /* GPZ_OK or the request's error */
+  uint32_t seg_size;        /* compress: the segment size used */
+  uint64_t stream_bytes;    /* compress: stream size */
+  void *d_out;              /* compress: the stream; decompress: x, y, z, n values each, every axis
+                               starting at a multiple of 256 bytes (stride: n * sizeof(T) rounded up to 256) */
+  double eb;                /* compress: the absolute bound used */
+  double queue_ms;          /* submit -> launch of its batch */
+  double total_ms;          /* submit -> completion seen by the server */
+  uint32_t batch_size;      /* requests in its batch */
+  uint32_t reserved;
+} gpz_completion;
+
+typedef struct gpz_server_stats {
+  uint64_t submitted, completed, batches, arena_bytes, arena_free_bytes;
+  uint32_t queued, in_flight;
+} gpz_server_stats;
+
+typedef struct gpz_server gpz_server;
+
+int gpz_server_create(const gpz_server_config *cfg, gpz_server **server);
+/* Never blocks.  GPZ_EINVAL for a malformed request, GPZ_ENOSPACE when its
+ * output could never fit in the arena. */
+int gpz_server_submit(gpz_server *server, const gpz_request *req, uint64_t *ticket);
+/* Blocks until the request completes (GPZ_ETIMEOUT after timeout_ms; 0 waits
+ * without limit). */
+int gpz_server_wait(gpz_server *server, uint64_t ticket, gpz_completion *out, uint32_t timeout_ms);
+/* Returns a completed request's output memory to the arena.  Requests are
+ * admitted in arrival order, so a caller that keeps outputs must release them
+ * for later requests to start once the arena is full. */
+int gpz_server_release(gpz_server *server, uint64_t ticket);
+int gpz_server_stats_get(gpz_server *server, gpz_server_stats *stats);
+/* Finishes the work in flight, then frees everything. */
+int gpz_server_destroy(gpz_server *server);
+
 /* Library version string. */
 const char *gpz_version(void);
 
