@@ -541,6 +541,121 @@ def run_batched(args):
     print(json.dumps(line), flush=True)
 
 
+SERVE_WORKLOAD = ("Poisson arrivals at the given rates, 70% compress / 30% decompress of previously produced "
+                  "streams, sizes log-uniform in [1e5, 5e7] points, 3D, 80% float32 / 20% float64, rel error "
+                  "bound drawn from {1e-3, 1e-4}; requests draw from a pool of 48 resident snapshots")
+
+
+def run_served(args):
+    """Served form: a request server (continuous batching, 120 GB budget)
+    against the plain per-request path (one synchronous call per request, in
+    arrival order) on the same Poisson arrival schedule.  Latency = arrival to
+    completion; GB/s = input bytes / (first arrival to last completion)."""
+    import math
+    import threading
+    import numpy as np
+    import torch
+    import gpz_b200 as gz
+    from gpz_b200.serve import Server
+    dev = torch.device("cuda", 0)
+    rng = np.random.default_rng(777)
+    pool = []
+    g = torch.Generator(device=dev)
+    for i in range(48):
+        n = int(round(math.exp(rng.uniform(math.log(1e5), math.log(5e7)))))
+        bits = 32 if rng.random() < 0.8 else 64
+        rel = (1e-3, 1e-4)[int(rng.integers(2))]
+        g.manual_seed(5000 + i)
+        L = 100.0 * (n / 1e6) ** (1.0 / 3)
+        dt = torch.float32 if bits == 32 else torch.float64
+        x, y, z = (torch.rand(n, generator=g, device=dev, dtype=dt) * L for _ in range(3))
+        eb, _ = gz.rel_to_abs(x, y, z, rel)
+        st, r = gz.compress(x, y, z, eb=eb, rel_mode=True, rel_eb=rel)
+        pool.append(dict(x=x, y=y, z=z, n=n, bits=bits, rel=rel, stream=st.clone(),
+                         header=gz.parse_header(st[:32].cpu().numpy().tobytes()), inb=3 * n * bits // 8))
+    torch.cuda.synchronize()
+    scr = torch.empty(gz.compress_scratch_bytes(max(p["n"] for p in pool)), dtype=torch.uint8, device=dev)
+    outc = torch.empty(max(gz.stream_bound(p["n"], 3, p["bits"]) for p in pool), dtype=torch.uint8, device=dev)
+    outd = [torch.empty(max(p["n"] for p in pool), dtype=torch.float64, device=dev) for _ in range(3)]
+    dscr = torch.empty(256, dtype=torch.uint8, device=dev)
+
+    def plain_one(req):
+        p = pool[req[1]]
+        if req[0] == "c":
+            eb, _ = gz.rel_to_abs(p["x"], p["y"], p["z"], p["rel"])
+            prm = gz.make_params(p["n"], 3, p["bits"], eb, 0, True, p["rel"])
+            r = gz.compress_into(prm, p["x"], p["y"], p["z"], outc, scr)
+            assert r.status == 0
+        else:
+            dt = torch.float32 if p["bits"] == 32 else torch.float64
+            o = [t.view(torch.uint8)[: p["n"] * p["bits"] // 8].view(dt) for t in outd]
+            r = gz.decompress_into(p["stream"], p["stream"].numel(), p["bits"], 3, o[0], o[1], o[2], dscr)
+            assert r.status == 0
+
+    results = {}
+    for rate in args.rates:
+        count = args.requests
+        arr = np.cumsum(rng.exponential(1.0 / rate, count))
+        reqs = [("c" if rng.random() < 0.7 else "d", int(rng.integers(len(pool)))) for _ in range(count)]
+        inb = sum(pool[k]["inb"] for _, k in reqs)
+        # ---- served
+        srv = Server(hbm_budget=120 << 30, streams=args.serve_streams, max_batch=64, overlap=args.overlap)
+        lat, tickets = [0.0] * count, [None] * count
+        done_at = [0.0] * count
+        t0 = time.perf_counter()
+
+        def consumer():
+            for i in range(count):
+                while tickets[i] is None:
+                    time.sleep(0.0001)
+                c = srv.wait(tickets[i], timeout_ms=600_000)
+                assert c.status == 0, c.status
+                done_at[i] = time.perf_counter()
+                lat[i] = c.total_ms
+                srv.release(tickets[i])
+
+        th = threading.Thread(target=consumer)
+        th.start()
+        for i, (op, k) in enumerate(reqs):
+            now = time.perf_counter() - t0
+            if arr[i] > now:
+                time.sleep(arr[i] - now)
+            p = pool[k]
+            if op == "c":
+                tickets[i] = srv.submit_compress(p["x"], p["y"], p["z"], rel_eb=p["rel"])
+            else:
+                tickets[i] = srv.submit_decompress(p["stream"], p["header"])
+        th.join()
+        span = max(done_at) - t0 - arr[0]
+        st = srv.stats()
+        srv.close()
+        # ---- plain: one synchronous call per request, in arrival order
+        platency = []
+        t0 = time.perf_counter()
+        for i, req in enumerate(reqs):
+            now = time.perf_counter() - t0
+            if arr[i] > now:
+                time.sleep(arr[i] - now)
+            plain_one(req)
+            platency.append((time.perf_counter() - t0 - arr[i]) * 1e3)
+        pspan = time.perf_counter() - t0 - arr[0]
+        results[str(rate)] = {
+            "requests": count, "input_bytes": inb,
+            "served": {"p50_ms": round(float(np.percentile(lat, 50)), 3), "p99_ms": round(float(np.percentile(lat, 99)), 3),
+                       "gbs": round(inb / span / 1e9, 2), "batches": int(st.batches),
+                       "mean_batch": round(count / max(1, st.batches), 2)},
+            "plain": {"p50_ms": round(float(np.percentile(platency, 50)), 3),
+                      "p99_ms": round(float(np.percentile(platency, 99)), 3), "gbs": round(inb / pspan / 1e9, 2)},
+        }
+    line = {"metric": "served p50/p99 latency (ms) and aggregate GB/s vs per-request calls, 1 B200", "unit": "ms",
+            "n_gpus": 1, "higher_is_better": False, "data": "synthetic",
+            "config": {"workload": SERVE_WORKLOAD, "hbm_budget_bytes": 120 << 30, "streams": args.serve_streams,
+                       "overlap": bool(args.overlap), "max_batch": 64,
+                       "pool_points": sum(p["n"] for p in pool)},
+            "rates": results}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -552,6 +667,12 @@ def main():
     ap.add_argument("--batched", action="store_true",
                     help="time the batched form (many snapshots per graph launch) against per-snapshot calls")
     ap.add_argument("--batch", type=int, default=256, help="snapshots in the batched workload")
+    ap.add_argument("--served", action="store_true",
+                    help="time the request server against per-request calls on a Poisson arrival schedule")
+    ap.add_argument("--rates", type=float, nargs="+", default=[50.0, 200.0, 800.0])
+    ap.add_argument("--requests", type=int, default=300, help="requests per arrival rate")
+    ap.add_argument("--serve-streams", type=int, default=2)
+    ap.add_argument("--overlap", action="store_true", help="let served batches run concurrently")
     ap.add_argument("--points", type=int, default=N_POINTS,
                     help="points per GPU (smaller cases for profiler captures; the headline uses the default)")
     args = ap.parse_args()
@@ -559,6 +680,8 @@ def main():
         run_reference(args)
     elif args.batched:
         run_batched(args)
+    elif args.served:
+        run_served(args)
     else:
         run_ours(args)
 

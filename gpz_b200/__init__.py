@@ -28,6 +28,7 @@ GPZ_FLAG_SAFE31 = 1
 GPZ_FLAG_SEG_FIXED = 2
 GPZ_FLAG_REL_ON_DEVICE = 4
 GPZ_OP_COMPRESS, GPZ_OP_DECOMPRESS = 1, 2
+GPZ_SERVER_OVERLAP = 1
 ERRORS = {1: "EINVAL", 2: "ESEG", 3: "ESTREAM", 4: "ENOSPACE", 5: "ECUDA", 6: "ETIMEOUT", 7: "ENOTSUP", 8: "ELIMIT"}
 
 
@@ -64,7 +65,7 @@ class BatchItem(ctypes.Structure):
 
 class ServerConfig(ctypes.Structure):
     _fields_ = [("hbm_budget", ctypes.c_uint64), ("streams", ctypes.c_uint32), ("max_batch", ctypes.c_uint32),
-                ("workspace_bytes", ctypes.c_uint64)]
+                ("workspace_bytes", ctypes.c_uint64), ("flags", ctypes.c_uint32), ("reserved", ctypes.c_uint32)]
 
 
 class Request(ctypes.Structure):

@@ -24,8 +24,8 @@ using namespace gpzb;
 
 namespace {
 
-constexpr uint64_t kRelPointsPerBlock = 1u << 16;  // points per rel->abs block of a snapshot
-constexpr uint64_t kRelMaxBlocks = 256;
+constexpr uint64_t kRelPointsPerBlock = 1u << 13;  // points per rel->abs block of a snapshot
+constexpr uint64_t kRelMaxBlocks = 1024;
 
 inline uint64_t align256(uint64_t v) { return (v + 255u) & ~255ull; }
 inline uint64_t chunks_of(uint64_t n) { return (n + kChunk - 1) / kChunk; }

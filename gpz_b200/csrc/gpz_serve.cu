@@ -176,6 +176,7 @@ struct gpz_server {
   std::unordered_map<uint64_t, Req> reqs;
   uint64_t next_ticket = 1, submitted = 0, completed = 0, batches = 0;
   uint64_t gen = 0;  // bumped by submit, release and stop: the worker's wake-up reasons
+  cudaEvent_t last = nullptr;  // completion event of the most recently launched batch
   bool stop = false;
   std::thread worker;
 
@@ -274,6 +275,8 @@ struct gpz_server {
         return false;
       }
     }
+    // without GPZ_SERVER_OVERLAP the GPU runs batches in launch order
+    if (!(cfg.flags & GPZ_SERVER_OVERLAP) && last) cudaStreamWaitEvent(s.st, last, 0);
     uint8_t *ws = arena.base + s.ws_off;
     uint8_t *wsd = ws + (ci.empty() ? 0 : up(Lc.bytes));
     uint8_t *img = s.image;
@@ -295,6 +298,7 @@ struct gpz_server {
     if (!di.empty())
       cudaMemcpyAsync(s.ctl_h + 2 * nc * kCtlBytes, wsd, di.size() * kCtlBytes, cudaMemcpyDeviceToHost, s.st);
     cudaEventRecord(s.done, s.st);
+    last = s.done;
     s.busy = true;
     ++batches;
     return true;
@@ -315,7 +319,7 @@ struct gpz_server {
       if (stop && pending.empty() && !any_busy) break;
       // batches in flight: poll their events; idle: sleep until a submit,
       // a release (the queue head may fit now) or stop
-      if (any_busy) cv_work.wait_for(lk, std::chrono::microseconds(50));
+      if (any_busy) cv_work.wait_for(lk, std::chrono::microseconds(20));
       else cv_work.wait(lk, [&] { return gen != seen; });
     }
   }
@@ -324,7 +328,9 @@ struct gpz_server {
 extern "C" {
 
 int gpz_server_create(const gpz_server_config *cfg, gpz_server **server) {
-  if (!cfg || !server || cfg->streams == 0 || cfg->max_batch == 0 || cfg->hbm_budget == 0) return GPZ_EINVAL;
+  if (!cfg || !server || cfg->streams == 0 || cfg->max_batch == 0 || cfg->hbm_budget == 0 ||
+      (cfg->flags & ~GPZ_SERVER_OVERLAP) != 0)
+    return GPZ_EINVAL;
   *server = nullptr;
   gpz_server *s = new (std::nothrow) gpz_server;
   if (!s) return GPZ_ECUDA;

@@ -17,8 +17,8 @@ import ctypes
 import threading
 
 from . import (Completion, GPZ_FLAG_REL_ON_DEVICE, GPZ_FLAG_SAFE31, GPZ_FLAG_SEG_FIXED, GPZ_OP_COMPRESS,
-               GPZ_OP_DECOMPRESS, GpzError, Request, ServerConfig, ServerStats, _check, _dtype_bits, lib,
-               parse_header)
+               GPZ_OP_DECOMPRESS, GPZ_SERVER_OVERLAP, GpzError, Request, ServerConfig, ServerStats, _check,
+               _dtype_bits, lib, parse_header)
 
 
 class _DeviceBuffer:
@@ -30,9 +30,10 @@ class _DeviceBuffer:
 
 
 class Server:
-    def __init__(self, hbm_budget: int, streams: int = 3, max_batch: int = 64, workspace_bytes: int = 0):
+    def __init__(self, hbm_budget: int, streams: int = 3, max_batch: int = 64, workspace_bytes: int = 0,
+                 overlap: bool = False):
         cfg = ServerConfig(hbm_budget=hbm_budget, streams=streams, max_batch=max_batch,
-                           workspace_bytes=workspace_bytes)
+                           workspace_bytes=workspace_bytes, flags=GPZ_SERVER_OVERLAP if overlap else 0, reserved=0)
         self._h = ctypes.c_void_p()
         _check(lib().gpz_server_create(ctypes.byref(cfg), ctypes.byref(self._h)), "gpz_server_create")
         self._keep = {}  # ticket -> (inputs kept alive until completion, output description)

@@ -310,7 +310,8 @@ int gpz_dbatch_destroy(gpz_dbatch *batch);
  * in batches on several CUDA streams (continuous batching): whenever a stream
  * is free, every queued request whose output fits in the device-memory budget
  * joins the next batch, so requests that arrive while others run are started
- * as soon as a stream and memory free up, and their work overlaps on the GPU.
+ * as soon as a stream and memory free up; their preparation and upload
+ * overlap the running batch, and with GPZ_SERVER_OVERLAP their kernels too.
  * All device memory -- request outputs and batch workspaces -- comes from one
  * arena of hbm_budget bytes allocated at creation; serving allocates nothing.
  * Outputs stay in the arena (device resident) until the caller releases them.
@@ -324,7 +325,17 @@ typedef struct gpz_server_config {
   uint32_t streams;         /* batches in flight at once, >= 1 */
   uint32_t max_batch;       /* requests per batch, >= 1 */
   uint64_t workspace_bytes; /* per stream: batch descriptors and control blocks (0: 64 MiB) */
+  uint32_t flags;           /* GPZ_SERVER_OVERLAP */
+  uint32_t reserved;        /* 0 */
 } gpz_server_config;
+
+/* Server flag: batches on different streams run concurrently on the GPU.
+ * Without it the GPU runs the batches one after another (each waits for the
+ * previous one's completion event) and the streams only let the server
+ * prepare and queue the next batches while one runs: two different codec
+ * kernels resident on one SM thrash its instruction cache, so concurrent
+ * batches are usually slower. */
+#define GPZ_SERVER_OVERLAP 1u
 
 typedef struct gpz_request {
   uint32_t op;              /* GPZ_OP_COMPRESS or GPZ_OP_DECOMPRESS */

@@ -31,7 +31,8 @@ def test_struct_layouts_match_the_header(tmp_path):
 @pytest.mark.parametrize("cfg", [dict(hbm_budget=1 << 30, streams=0, max_batch=4, workspace_bytes=0),
                                  dict(hbm_budget=1 << 30, streams=2, max_batch=0, workspace_bytes=0),
                                  dict(hbm_budget=0, streams=2, max_batch=4, workspace_bytes=0),
-                                 dict(hbm_budget=1 << 20, streams=2, max_batch=4, workspace_bytes=1 << 20)])
+                                 dict(hbm_budget=1 << 20, streams=2, max_batch=4, workspace_bytes=1 << 20),
+                                 dict(hbm_budget=1 << 30, streams=2, max_batch=4, workspace_bytes=0, flags=6)])
 def test_server_create_rejects_bad_configs_before_touching_the_gpu(cfg):
     h = ctypes.c_void_p()
     assert gz.lib().gpz_server_create(ctypes.byref(gz.ServerConfig(**cfg)), ctypes.byref(h)) == gz.GPZ_EINVAL
@@ -66,14 +67,16 @@ def _single_compress(x, y, z, kw):
 
 
 @pytest.mark.gpu
-def test_requests_in_a_mix_equal_single_calls():
+@pytest.mark.parametrize("overlap", [False, True])
+def test_requests_in_a_mix_equal_single_calls(overlap):
     """Compress and decompress requests submitted together (batched across
-    three streams) give the single-call bytes and reconstructions."""
+    three streams, run in order or concurrently) give the single-call bytes
+    and reconstructions."""
     import torch
     from gpz_b200.serve import Server
     ins = _inputs()
     singles = [_single_compress(x, y, z, kw) for x, y, z, kw in ins]
-    srv = Server(hbm_budget=2 << 30, streams=3, max_batch=4)
+    srv = Server(hbm_budget=2 << 30, streams=3, max_batch=4, overlap=overlap)
     try:
         tickets = []
         for (x, y, z, kw), (s, _) in zip(ins, singles):
