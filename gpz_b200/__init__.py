@@ -89,6 +89,13 @@ class ServerStats(ctypes.Structure):
                 ("queued", ctypes.c_uint32), ("in_flight", ctypes.c_uint32)]
 
 
+class VerifyResult(ctypes.Structure):
+    _fields_ = [("points", ctypes.c_uint64), ("over_bound", ctypes.c_uint64), ("over_bound_tol", ctypes.c_uint64),
+                ("max_abs_err", ctypes.c_double * 3), ("mse", ctypes.c_double * 3),
+                ("value_range", ctypes.c_double * 3), ("psnr", ctypes.c_double * 3),
+                ("psnr_combined", ctypes.c_double)]
+
+
 class DBatchItem(ctypes.Structure):
     """gpz_dbatch_item: one stream of a batched decompress."""
     _fields_ = [("d_stream", ctypes.c_void_p), ("stream_bytes", ctypes.c_uint64), ("float_bits", ctypes.c_uint32),
@@ -141,6 +148,9 @@ SIGNATURES = {
     "gpz_server_release": (ctypes.c_int, [_VP, _U64]),
     "gpz_server_stats_get": (ctypes.c_int, [_VP, ctypes.POINTER(ServerStats)]),
     "gpz_server_destroy": (ctypes.c_int, [_VP]),
+    "gpz_verify_scratch_bytes": (_U64, []),
+    "gpz_verify": (ctypes.c_int, [_U32, _U32, _U64, _VP, _VP, _VP, _VP, _VP, _VP, ctypes.c_double, _U32, _VP, _U64,
+                                  ctypes.POINTER(VerifyResult), _VP]),
 }
 
 _lib = None
@@ -293,6 +303,22 @@ def rel_to_abs(x, y, z, rel: float, stream=None):
                               rel, scratch.data_ptr(), 256, ctypes.byref(eb), mm, _stream_ptr(stream))
     _check(rc, "gpz_rel_to_abs")
     return eb.value, list(mm)
+
+
+def verify(x, y, z, rx, ry, rz, eb: float, seg_size: int, stream=None) -> "VerifyResult":
+    """Per-point check of a reconstruction (stream order, as decompress
+    returns it) against the original SoA tensors; eb and seg_size as in the
+    stream header."""
+    torch = _torch()
+    dim = 3 if z is not None else 2
+    scratch = torch.empty(int(lib().gpz_verify_scratch_bytes()), dtype=torch.uint8, device=x.device)
+    res = VerifyResult()
+    rc = lib().gpz_verify(_dtype_bits(x), dim, x.numel(), x.data_ptr(), y.data_ptr(),
+                          z.data_ptr() if dim == 3 else None, rx.data_ptr(), ry.data_ptr(),
+                          rz.data_ptr() if dim == 3 else None, float(eb), int(seg_size), scratch.data_ptr(),
+                          scratch.numel(), ctypes.byref(res), _stream_ptr(stream))
+    _check(rc, "gpz_verify")
+    return res
 
 
 # ---------------------------------------------------------------------------

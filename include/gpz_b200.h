@@ -389,6 +389,33 @@ int gpz_server_stats_get(gpz_server *server, gpz_server_stats *stats);
 /* Finishes the work in flight, then frees everything. */
 int gpz_server_destroy(gpz_server *server);
 
+/* ---- verification -------------------------------------------------------------------
+ * Replaces the reference's verifier (src/utils.cu:17-217, used by the CLI's
+ * -v), which sorts every axis of the original and of the reconstruction and
+ * compares the sorted sequences, so it never pairs a point with its own
+ * reconstruction.  gpz_verify recovers the exact pairing on the device: per
+ * 1024-point chunk it recomputes the encoder's sort of the points by block
+ * (from the originals, eb and seg_size, as found in the stream header), so
+ * reconstructed point s of the chunk is compared with the original the
+ * encoder placed at s.  Inputs: the original SoA arrays and the
+ * reconstruction in stream order (gpz_decompress's output).  Synchronises
+ * `stream`; needs gpz_verify_scratch_bytes() of scratch. */
+typedef struct gpz_verify_result {
+  uint64_t points;
+  uint64_t over_bound;      /* points with some axis |reconstruction - original| > eb */
+  uint64_t over_bound_tol;  /* ... > 1.01 * eb (the reference verifier's tolerance) */
+  double max_abs_err[3];
+  double mse[3];
+  double value_range[3];    /* max - min of the originals */
+  double psnr[3];           /* 20 log10(range) - 10 log10(mse), per axis */
+  double psnr_combined;     /* from the per-axis normalised RMS errors, as the reference CLI combines them */
+} gpz_verify_result;
+
+uint64_t gpz_verify_scratch_bytes(void);
+int gpz_verify(uint32_t float_bits, uint32_t dim, uint64_t n, const void *d_x, const void *d_y, const void *d_z,
+               const void *d_rx, const void *d_ry, const void *d_rz, double eb, uint32_t seg_size, void *d_scratch,
+               uint64_t scratch_bytes, gpz_verify_result *result, void *stream);
+
 /* Library version string. */
 const char *gpz_version(void);
 
