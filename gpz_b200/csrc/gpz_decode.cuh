@@ -396,7 +396,7 @@ __device__ __forceinline__ void decode_chunk(const DArgs<T> &a, unsigned long lo
   }
   uint32_t *const A = sw + Cfg::A;
 #pragma unroll
-  for (int m = 0; m < 8; ++m) reinterpret_cast<uint4 *>(A + 32 * lane)[m] = make_uint4(0u, 0u, 0u, 0u);
+  for (int m = 0; m < 8; ++m) *reinterpret_cast<uint4 *>(A + qoff(lane, m)) = make_uint4(0u, 0u, 0u, 0u);  // swizzled: no bank conflicts
 
   // ---- counts -> run starts as 16-bit pairs P16[k] = st_k | st_{k+16} << 16 ----
   uint32_t P16[16];

@@ -272,7 +272,7 @@ static __device__ __noinline__ void rank_wide(uint32_t *sw, uint32_t kmin, uint3
   // wider composites: 2048 buckets on the top bits, S keeps the bits below
   const uint32_t shb = cbits_all - kEncBucketBits;
 #pragma unroll
-  for (int m = 0; m < 8; ++m) reinterpret_cast<uint4 *>(hist + 32 * lane)[m] = make_uint4(0u, 0u, 0u, 0u);
+  for (int m = 0; m < 8; ++m) *reinterpret_cast<uint4 *>(hist + qoff(lane, m)) = make_uint4(0u, 0u, 0u, 0u);
   __syncwarp();
   uint32_t bs[32];  // bucket << 10 | arrival slot
   auto count_pass = [&](auto wide_c) {
@@ -394,7 +394,7 @@ static __device__ __noinline__ void rank_wide(uint32_t *sw, uint32_t kmin, uint3
       const uint32_t next0 = __shfl_down_sync(FULL, st2[0] & 0xFFFFu, 1);
       __syncwarp();
 #pragma unroll
-      for (int m = 0; m < 8; ++m) reinterpret_cast<uint4 *>(hist + 32 * lane)[m] = make_uint4(0u, 0u, 0u, 0u);
+      for (int m = 0; m < 8; ++m) *reinterpret_cast<uint4 *>(hist + qoff(lane, m)) = make_uint4(0u, 0u, 0u, 0u);
       __syncwarp();
 #pragma unroll
       for (int k = 0; k < 32; ++k) {
