@@ -148,8 +148,7 @@ __global__ void __launch_bounds__(32 * kEncWarps, GPZ_ENC_MIN_CTAS)
       if (pay_base + off + payload > a.out_cap) {
         if (lane == 0) set_status(ctl, kENOSPACE);
       } else {
-        uint32_t *dst = reinterpret_cast<uint32_t *>(a.out + pay_base + off);
-        for (uint32_t w = lane; w < payload / 4u; w += 32) dst[w] = sw[w];
+        copy_payload(reinterpret_cast<uint32_t *>(a.out + pay_base + off), sw, payload, lane);
       }
       if (c == G - 1 && lane == 0) ctl->stream_bytes = pay_base + off + payload;
     }
