@@ -149,6 +149,7 @@ SIGNATURES = {
     "gpz_server_stats_get": (ctypes.c_int, [_VP, ctypes.POINTER(ServerStats)]),
     "gpz_server_destroy": (ctypes.c_int, [_VP]),
     "gpz_verify_scratch_bytes": (_U64, []),
+    "gpz_selftest_lookback_timeout": (ctypes.c_int, [_U32, _VP, _U64, ctypes.POINTER(ctypes.c_int32), _VP]),
     "gpz_verify": (ctypes.c_int, [_U32, _U32, _U64, _VP, _VP, _VP, _VP, _VP, _VP, ctypes.c_double, _U32, _VP, _U64,
                                   ctypes.POINTER(VerifyResult), _VP]),
 }

@@ -504,3 +504,33 @@ int gpz_compress_noalloc(const gpz_params *params, const void *d_x, const void *
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Check of the bounded wait of the placement look-back: group 1 waits on a
+// group 0 that never publishes its size (its look-back word stays zero, as if
+// the CTA holding it had stopped), so the wait runs out after `polls` polls.
+// ---------------------------------------------------------------------------
+namespace {
+__global__ void lookback_timeout_kernel(unsigned long long *look, Control *ctl, uint32_t polls) {
+  unsigned long long excl = 0;
+  const bool ok = resolve_prefix(look, 1ull, 0ull, ctl, excl, polls);
+  if (threadIdx.x == 0) ctl->stream_bytes = ok ? 1ull : 0ull;
+}
+}  // namespace
+
+extern "C" int gpz_selftest_lookback_timeout(uint32_t polls, void *d_scratch, uint64_t scratch_bytes, int32_t *status,
+                                             void *stream) {
+  if (!d_scratch || !status || polls == 0 || polls > kSpinLimit) return GPZ_EINVAL;
+  if (scratch_bytes < kCtlBytes + 16) return GPZ_ENOSPACE;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  Control *ctl = static_cast<Control *>(d_scratch);
+  unsigned long long *look = reinterpret_cast<unsigned long long *>(static_cast<uint8_t *>(d_scratch) + kCtlBytes);
+  if (cudaMemsetAsync(d_scratch, 0, kCtlBytes + 16, st) != cudaSuccess) return GPZ_ECUDA;
+  lookback_timeout_kernel<<<1, 32, 0, st>>>(look, ctl, polls);
+  if (cudaGetLastError() != cudaSuccess) return GPZ_ECUDA;
+  Control h;
+  if (cudaMemcpyAsync(&h, d_scratch, sizeof(h), cudaMemcpyDeviceToHost, st) != cudaSuccess) return GPZ_ECUDA;
+  if (cudaStreamSynchronize(st) != cudaSuccess) return GPZ_ECUDA;
+  *status = h.status;
+  return GPZ_OK;
+}

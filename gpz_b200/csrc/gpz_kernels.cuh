@@ -408,10 +408,11 @@ __device__ __forceinline__ void publish_aggregate(unsigned long long *look, unsi
   st_relaxed(&look[c], (c == 0 ? kFlagInc : kFlagAgg) | agg);
 }
 
-// Warp-collective.  Returns false when a bounded wait gave up or another CTA
-// aborted (the kernel then stops taking chunks and reports GPZ_ETIMEOUT).
+// Warp-collective.  Returns false when a bounded wait (`limit` polls of a
+// predecessor that has published nothing) gave up or another CTA aborted (the
+// kernel then stops taking chunks and reports GPZ_ETIMEOUT).
 static __device__ bool resolve_prefix(unsigned long long *look, unsigned long long c, unsigned long long agg,
-                               Control *ctl, unsigned long long &excl_out) {
+                                      Control *ctl, unsigned long long &excl_out, uint32_t limit = kSpinLimit) {
   const int lane = threadIdx.x & 31;
   if (c == 0) {
     excl_out = 0;
@@ -428,7 +429,7 @@ static __device__ bool resolve_prefix(unsigned long long *look, unsigned long lo
     const uint32_t mNone = __ballot_sync(0xFFFFFFFFu, fl == 0u);
     const uint32_t need = mInc ? (((mInc & (0u - mInc)) << 1) - 1u) : 0xFFFFFFFFu;
     if (mNone & need) {
-      if (++spins > kSpinLimit || ld_volatile(&ctl->abort)) {
+      if (++spins > limit || ld_volatile(&ctl->abort)) {
         if (lane == 0) {
           atomicExch(&ctl->abort, 1u);
           set_status(ctl, kETIMEOUT);

@@ -416,6 +416,19 @@ int gpz_verify(uint32_t float_bits, uint32_t dim, uint64_t n, const void *d_x, c
                const void *d_rx, const void *d_ry, const void *d_rz, double eb, uint32_t seg_size, void *d_scratch,
                uint64_t scratch_bytes, gpz_verify_result *result, void *stream);
 
+/* ---- self-test of the bounded waits ---------------------------------------------
+ * No counterpart in the reference (its placement is a separate CUB scan, with
+ * no waiting between blocks).  The compress kernels place chunks with a
+ * decoupled look-back whose every wait is bounded: after a limited number of
+ * polls of a predecessor that has published nothing, the kernel sets
+ * GPZ_ETIMEOUT and returns, so a stuck predecessor cannot hang the GPU.  This
+ * runs that wait against a predecessor that never publishes, with `polls`
+ * (1 .. 4,194,304) as the limit, and returns the status the kernel recorded
+ * (GPZ_ETIMEOUT when the wait ran out).  Needs gpz_compress_scratch_bytes(2048)
+ * of scratch; synchronises `stream`. */
+int gpz_selftest_lookback_timeout(uint32_t polls, void *d_scratch, uint64_t scratch_bytes, int32_t *status,
+                                  void *stream);
+
 /* Library version string. */
 const char *gpz_version(void);
 
