@@ -128,6 +128,19 @@ __device__ __forceinline__ unsigned long long warp_max(unsigned long long v) {
   return ((unsigned long long)hi << 32) | lo;
 }
 
+// Three-source float min / max (sm_100's min.f32 / max.f32 with three inputs):
+// the same result as two two-input fminf / fmaxf, NaN sources ignored.
+__device__ __forceinline__ float fmin3f(float a, float b, float c) {
+  float r;
+  asm("min.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(a), "f"(b), "f"(c));
+  return r;
+}
+__device__ __forceinline__ float fmax3f(float a, float b, float c) {
+  float r;
+  asm("max.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(a), "f"(b), "f"(c));
+  return r;
+}
+
 __device__ __forceinline__ uint32_t bitlen(uint32_t v) { return 32u - (uint32_t)__clz(v); }
 __device__ __forceinline__ uint32_t bitlen64(unsigned long long v) { return 64u - (uint32_t)__clzll(v); }
 

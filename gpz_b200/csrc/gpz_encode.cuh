@@ -439,6 +439,12 @@ static __device__ __noinline__ void rank_wide(uint32_t *sw, uint32_t kmin, uint3
 // axes in registers (element j of lane l is point 32j + l of the chunk), so a
 // chunk costs one round of loads and the next chunk's loads overlap the
 // current one's placement.  Double streams load one axis at a time.
+//
+// The slots past the end of a short last chunk hold a copy of the chunk's
+// first point: they leave the chunk's min / max, id range and largest
+// relative position unchanged, so the encoder's per-point loops need no
+// validity test and only the ranking and the relative-position section treat
+// those slots specially.
 template <typename T, int DIM>
 struct ChunkPoints {
   static constexpr bool kAhead = sizeof(T) == 4;
@@ -460,7 +466,7 @@ struct ChunkPoints {
 #pragma unroll
           for (int j = 0; j < 32; ++j) {
             const uint32_t p = 32u * j + lane;
-            v[d][j] = p < nvalid ? X[d][base + p] : (T)0;
+            v[d][j] = X[d][base + (p < nvalid ? p : 0u)];
           }
       }
     }
@@ -501,7 +507,7 @@ __device__ __forceinline__ uint32_t encode_chunk(const CArgs<T> &a, unsigned lon
 #pragma unroll
       for (int j = 0; j < 32; ++j) {
         const uint32_t p = 32u * j + lane;
-        vl[j] = (full || p < nvalid) ? src[p] : (T)0;
+        vl[j] = (full || p < nvalid) ? src[p] : src[0];  // past the end: the first point
       }
     }
     auto vv_of = [&](int j) -> T {
@@ -509,12 +515,19 @@ __device__ __forceinline__ uint32_t encode_chunk(const CArgs<T> &a, unsigned lon
       else return vl[j];
     };
     // fmin / fmax ignore NaN and order -0.0 below +0.0, as the reference's
-    // warp reductions do (:122-139)
+    // warp reductions do (:122-139); slots past the end repeat a point
     const T lim = is64 ? (T)DBL_MAX : (T)FLT_MAX;
     T mn = lim, mx = -lim;
+    if constexpr (!is64) {
 #pragma unroll
-    for (int j = 0; j < 32; ++j)
-      if (full || 32u * j + lane < nvalid) { mn = fmin(mn, vv_of(j)); mx = fmax(mx, vv_of(j)); }
+      for (int j = 0; j < 32; j += 2) {
+        mn = fmin3f(mn, vv_of(j), vv_of(j + 1));
+        mx = fmax3f(mx, vv_of(j), vv_of(j + 1));
+      }
+    } else {
+#pragma unroll
+      for (int j = 0; j < 32; ++j) { mn = fmin(mn, vv_of(j)); mx = fmax(mx, vv_of(j)); }
+    }
     mn = from_ord((UO)~warp_max((UO)~ord_of(mn)));
     mx = from_ord(warp_max(ord_of(mx)));
     mm[d] = mn;
@@ -558,7 +571,7 @@ __device__ __forceinline__ uint32_t encode_chunk(const CArgs<T> &a, unsigned lon
 #pragma unroll
         for (int e = 0; e < 4; ++e) {
           rq[e] &= 0x7FFFFFFFu;
-          if (full || 32u * (4 * m + e) + lane < nvalid) rmax = max(rmax, rq[e]);
+          rmax = max(rmax, rq[e]);
         }
       }
       *row = make_uint4(rq[0], rq[1], rq[2], rq[3]);
@@ -585,7 +598,8 @@ __device__ __forceinline__ uint32_t encode_chunk(const CArgs<T> &a, unsigned lon
 #pragma unroll
   for (int j = 0; j < 32; ++j) {
     key[j] &= 0x7FFFFFFFu;
-    if (full || 32u * j + lane < nvalid) { kmin = min(kmin, key[j]); kmax = max(kmax, key[j]); }
+    kmin = min(kmin, key[j]);
+    kmax = max(kmax, key[j]);
   }
   kmin = warp_min(kmin);
   kmax = warp_max(kmax);
@@ -597,17 +611,24 @@ __device__ __forceinline__ uint32_t encode_chunk(const CArgs<T> &a, unsigned lon
   const uint32_t cbits_all = bitlen64(cmax);
   uint32_t rp[16];  // rank r of positions j and j+16 (16-bit pairs)
   if (cbits_all <= 32u) {
-    // 32-bit composites: one data-independent warp sort; points past the
-    // chunk's end hold the maximum and sort last
+    // 32-bit composites: one data-independent warp sort.  Slots past the
+    // chunk's end take the largest composite, (kmax - kmin) << 10 | 1023: no
+    // point of a short chunk has r = 1023, so they sort last, and they carry
+    // the last id kmax, so they start no run.
 #pragma unroll
     for (int m = 0; m < 8; ++m) {
       uint32_t cv[4];
 #pragma unroll
       for (int e = 0; e < 4; ++e) {
         const int j = 4 * m + e;
-        cv[e] = (full || 32u * j + lane < nvalid) ? (((key[j] - kmin) << 10) | (32u * lane + j)) : FULL;
+        cv[e] = ((key[j] - kmin) << 10) | (32u * lane + j);
       }
       *reinterpret_cast<uint4 *>(S + qoff(lane, m)) = make_uint4(cv[0], cv[1], cv[2], cv[3]);
+    }
+    if (!full) {
+#pragma unroll 1
+      for (int j = 0; j < 32; ++j)
+        if (32u * j + lane >= nvalid) S[qoff(lane, j >> 2) + (j & 3)] = (uint32_t)cmax;
     }
     warp_sort1024_rows(S, hist, lane);
 #pragma unroll
@@ -631,6 +652,10 @@ __device__ __forceinline__ uint32_t encode_chunk(const CArgs<T> &a, unsigned lon
       const uint4 t = *reinterpret_cast<const uint4 *>(S + qoff(lane, m));
       key[4 * m] = t.x; key[4 * m + 1] = t.y; key[4 * m + 2] = t.z; key[4 * m + 3] = t.w;
     }
+    if (!full) {  // positions past the end carry the last id: they start no run
+#pragma unroll
+      for (int j = 0; j < 32; ++j) key[j] = 32u * lane + j < nvalid ? key[j] : kmax;
+    }
 #pragma unroll
     for (int m = 0; m < 4; ++m) {
       const uint4 t = *reinterpret_cast<const uint4 *>(hist + qoff(lane, m));
@@ -649,7 +674,7 @@ __device__ __forceinline__ uint32_t encode_chunk(const CArgs<T> &a, unsigned lon
     for (int j = 0; j < 32; ++j) {
       const uint32_t pos = 32u * lane + j;
       const uint32_t pk = j ? key[j - 1] : prevk;
-      const bool st = pos < nvalid && (pos == 0 || key[j] != pk);
+      const bool st = pos == 0 || key[j] != pk;  // positions past the end repeat kmax
       if (st) {
         fm |= 1u << j;
         dm = max(dm, pos == 0 ? 0u : bitlen(key[j] - pk));
@@ -720,8 +745,13 @@ __device__ __forceinline__ uint32_t encode_chunk(const CArgs<T> &a, unsigned lon
   // delta + count sections end below 8 KB: the rank rows are still intact
 #pragma unroll
   for (int j = 0; j < 32; ++j) {
-    const uint32_t r = (rp[j & 15] >> (16 * (j >> 4))) & 0xFFFFu;
-    dl[j] = 32u * lane + j < nvalid ? relR[sx(r)] : 0xFFFFFFFFu;  // invalid slots (:197)
+    const uint32_t r = (rp[j & 15] >> (16 * (j >> 4))) & 1023u;
+    dl[j] = relR[sx(r)];
+  }
+  if (!full) {
+#pragma unroll
+    for (int j = 0; j < 32; ++j)
+      if (32u * lane + j >= nvalid) dl[j] = 0xFFFFFFFFu;  // slots past the end (:197)
   }
   __syncwarp();
   put_planes(stage, db + cb, rbits, 0u, dl, lane);
