@@ -668,16 +668,30 @@ __device__ __forceinline__ uint32_t encode_chunk(const CArgs<T> &a, unsigned lon
   uint32_t *const runStart = sw, *const deltaA = sw + kChunk;
   uint32_t U, dbits, cbits, first;
   {
+    // ids ascend, so a run starts where the id differs from its predecessor,
+    // and the widest delta is the bit length of all deltas ORed together;
+    // position 0 starts the first run with delta 0.  Positions past the end
+    // repeat kmax and start no run.
     const uint32_t prevk = __shfl_up_sync(FULL, key[31], 1);
-    uint32_t fm = 0, dm = 0;
+    const uint32_t pk0 = lane == 0 ? key[0] : prevk;
+    uint32_t fm = lane == 0 ? 1u : 0u, dm = 0;
+    if constexpr (!is64) {
+      uint32_t dor = 0;
 #pragma unroll
-    for (int j = 0; j < 32; ++j) {
-      const uint32_t pos = 32u * lane + j;
-      const uint32_t pk = j ? key[j - 1] : prevk;
-      const bool st = pos == 0 || key[j] != pk;  // positions past the end repeat kmax
-      if (st) {
-        fm |= 1u << j;
-        dm = max(dm, pos == 0 ? 0u : bitlen(key[j] - pk));
+      for (int j = 0; j < 32; ++j) {
+        const uint32_t dlt = key[j] - (j ? key[j - 1] : pk0);
+        dor |= dlt;
+        if (dlt != 0u) fm |= 1u << j;
+      }
+      dm = bitlen(dor);
+    } else {  // the same result; this form keeps the double kernels' registers lower
+#pragma unroll
+      for (int j = 0; j < 32; ++j) {
+        const uint32_t dlt = key[j] - (j ? key[j - 1] : pk0);
+        if (dlt != 0u) {
+          fm |= 1u << j;
+          dm = max(dm, bitlen(dlt));
+        }
       }
     }
     const uint32_t cnt = __popc(fm);
@@ -694,10 +708,8 @@ __device__ __forceinline__ uint32_t encode_chunk(const CArgs<T> &a, unsigned lon
 #pragma unroll
     for (int j = 0; j < 32; ++j) {
       if ((fm >> j) & 1u) {
-        const uint32_t pos = 32u * lane + j;
-        const uint32_t pk = j ? key[j - 1] : prevk;
-        runStart[sx(u)] = pos;
-        deltaA[sx(u)] = pos == 0 ? 0u : key[j] - pk;
+        runStart[sx(u)] = 32u * lane + j;
+        deltaA[sx(u)] = key[j] - (j ? key[j - 1] : pk0);
         ++u;
       }
     }
