@@ -35,7 +35,8 @@ def _cuda():
 
 
 def _t(a):
-    return torch.from_numpy(np.ascontiguousarray(a)).cuda()
+    a = np.ascontiguousarray(a)
+    return torch.from_numpy(a if a.flags.writeable else a.copy()).cuda()
 
 
 def _typed(bits, v):
@@ -67,6 +68,10 @@ def _check_roundtrip(stream, dim, bits):
 
 def run_case(kind, n, dim, bits, lo, hi, seed, mode, e, seg_in, special=None, safe31=False):
     x, y, z = mg.make_input(kind, n, dim, bits, lo, hi, seed, special)
+    return run_arrays(x, y, z, dim, bits, mode, e, seg_in, safe31)
+
+
+def run_arrays(x, y, z, dim, bits, mode, e, seg_in, safe31=False):
     ebT, relT, seg, adj, s_o = _oracle_case(x, y, z, dim, bits, mode, e, seg_in, safe31)
     s_g, r = _gpu_compress(x, y, z, dim, ebT, seg_in, mode, relT, safe31)
     assert r.status == 0
@@ -132,6 +137,30 @@ EDGE = [
 @pytest.mark.parametrize("case", EDGE, ids=[f"{c[0]}-{c[1]}-{c[2]}d-f{c[3]}-{c[7]}{c[8]}-s{c[9]}" for c in EDGE])
 def test_edge_cases_bit_exact(case):
     run_case(*case)
+
+
+@pytest.mark.parametrize("mode,e,seg", [("abs", 0.05, 8), ("rel", 1e-4, 0)])
+@pytest.mark.parametrize("bits,dim", [(32, 3), (32, 2), (64, 3), (64, 2)])
+def test_nan_points_bit_exact(bits, dim, mode, e, seg):
+    """NaN coordinates are ignored by the chunk min/max and quantize to 0 (the
+    GPU's min/max and saturating conversion); signed zeros order -0.0 below
+    +0.0.  Covered: NaNs scattered over whole chunks, a chunk whose first
+    point is NaN, a short last chunk whose first point (the one its unused
+    slots repeat) is NaN, and a chunk whose x axis is NaN throughout."""
+    dtype = np.float32 if bits == 32 else np.float64
+    n = 6 * 1024 + 300
+    x, y, z = po.generate(0, n, dim, 0.0, 100.0, 21, dtype)
+    rng = np.random.default_rng(5)
+    for a in (x, y, z):
+        a[rng.choice(n, 60, replace=False)] = np.nan
+    x[1024] = np.nan                  # first point of chunk 1
+    y[6 * 1024] = np.nan              # first point of the short last chunk
+    x[6 * 1024 + 1] = -0.0
+    x[6 * 1024 + 2] = 0.0
+    x[3 * 1024:4 * 1024] = np.nan     # chunk 3: no x value at all
+    if dim == 2:
+        z[:] = 0
+    run_arrays(x, y, z, dim, bits, mode, e, seg)
 
 
 @pytest.mark.parametrize("heavy", [17, 90, 300, 1023])
