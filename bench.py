@@ -226,35 +226,25 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
-def run_e2e(args, world, p, hx, hy, hz, n, cap, out, scr_c, scr_d, ox, oy, oz, dev, inb):
-    """Compress + decompress through the C ABI from / to pinned host buffers, every copy timed."""
+def run_e2e(args, world, p, hx, hy, hz, n, dev, inb, ref_out):
+    """Compress + decompress through the C ABI from and to pinned host buffers,
+    every copy timed.  Consecutive steps overlap their copies
+    (gpz_b200.pipeline.SnapshotPipeline): each step uploads the snapshot,
+    downloads its stream, uploads the stream again and downloads the
+    reconstruction.  The last step's host reconstruction must equal the
+    device-resident one."""
     import torch
-    import gpz_b200 as gz
-    hs = torch.empty(cap, dtype=torch.uint8).pin_memory()
-    rx, ry, rz = (torch.empty(n, dtype=torch.float32).pin_memory() for _ in range(3))
-    dx, dy, dz = (torch.empty(n, dtype=torch.float32, device=dev) for _ in range(3))
-    d_in = torch.empty(cap, dtype=torch.uint8, device=dev)
-
-    def e2e_step():
-        for h, d in ((hx, dx), (hy, dy), (hz, dz)):
-            d.copy_(h, non_blocking=True)
-        rc = gz.compress_into(p, dx, dy, dz, out, scr_c)  # reads back the result (size, status)
-        nb = int(rc.stream_bytes)
-        hs[:nb].copy_(out[:nb], non_blocking=True)
-        d_in[:nb].copy_(hs[:nb], non_blocking=True)
-        gz.decompress_into(d_in, nb, 32, 3, ox, oy, oz, scr_d, sync=False)
-        for d, h in ((ox, rx), (oy, ry), (oz, rz)):
-            h.copy_(d, non_blocking=True)
-        torch.cuda.synchronize()
-        return nb
-
-    e2e_steps = max(1, min(args.steps, 3))
-    e2e_step()
+    from gpz_b200.pipeline import SnapshotPipeline
+    pipe = SnapshotPipeline(p, n, 3, 32, dev)
+    e2e_steps = max(2, min(args.steps, 6))
+    pipe.round_trips([hx, hy, hz], 2)  # warm-up
     barrier(world)
     te0 = time.perf_counter()
-    for _ in range(e2e_steps):
-        nb = e2e_step()
+    nb, rx = pipe.round_trips([hx, hy, hz], e2e_steps)
     te1 = time.perf_counter()
+    for h, d in zip(rx, ref_out):
+        if not torch.equal(h, d.cpu()):
+            raise RuntimeError("end-to-end reconstruction differs from the device-resident one")
     e2e_ms = max_over_ranks((te1 - te0) * 1e3 / e2e_steps, world)
     return world * inb / (e2e_ms * 1e-3) / 1e9, nb, e2e_steps
 
@@ -334,7 +324,7 @@ def run_ours(args):
     if args.no_e2e:
         e2e_val, nb, e2e_steps = None, sbytes, 0
     else:
-        e2e_val, nb, e2e_steps = run_e2e(args, world, p, hx, hy, hz, n, cap, out, scr_c, scr_d, ox, oy, oz, dev, inb)
+        e2e_val, nb, e2e_steps = run_e2e(args, world, p, hx, hy, hz, n, dev, inb, (ox, oy, oz))
 
     cpu = None
     if world == 1 and rank == 0 and not args.no_cpu_baseline:

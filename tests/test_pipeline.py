@@ -1,0 +1,41 @@
+"""Host-memory round trips with overlapped copies (gpz_b200.pipeline): the
+stream and reconstruction of every step equal the single-call ones."""
+import numpy as np
+import pytest
+
+import gpz_b200 as gz
+from gpz_b200.pipeline import SnapshotPipeline
+
+
+def test_rejects_bad_shapes_before_allocating():
+    for dim, bits in ((4, 32), (3, 16), (1, 64)):
+        with pytest.raises(gz.GpzError):
+            SnapshotPipeline(gz.make_params(1000, 3, 32, 0.1), 1000, dim, bits)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("n,dim,bits,steps,abs_eb", [(300_000, 3, 32, 3, 0.0), (70_001, 2, 64, 4, 0.0),
+                                                     (1, 3, 32, 2, 0.01)])
+def test_round_trips_equal_single_calls(n, dim, bits, steps, abs_eb):
+    import torch
+    from oracle import pyoracle as po
+    dt = np.float32 if bits == 32 else np.float64
+    x, y, z = po.generate(1, n, dim, 0.0, 500.0, 31, dt)
+    dev = [torch.from_numpy(a.copy()).cuda() for a in (x, y, z)]
+    zz = dev[2] if dim == 3 else None
+    if abs_eb:  # one point has no range for a relative bound
+        eb, rel, seg = abs_eb, 0.0, 4
+    else:
+        (eb, _), rel, seg = gz.rel_to_abs(dev[0], dev[1], zz, 1e-4), float(dt(1e-4)), 0
+    want, r = gz.compress(dev[0], dev[1], zz, eb=eb, seg_size=seg, rel_mode=not abs_eb, rel_eb=rel)
+    wx, wy, wz = gz.decompress(want)
+    host = [torch.from_numpy(a.copy()).pin_memory() for a in (x, y, z)][:dim]
+    p = gz.make_params(n, dim, bits, eb, seg, not abs_eb, rel)
+    pipe = SnapshotPipeline(p, n, dim, bits)
+    nb, rx = pipe.round_trips(host, steps)
+    assert nb == r.stream_bytes
+    for k in range(2):
+        if pipe.nb[k]:
+            assert torch.equal(pipe.hs[k][:nb].cuda(), want)
+    for h, w in zip(rx, (wx, wy, wz)):
+        assert torch.equal(h.view(torch.uint8), w.cpu().view(torch.uint8))
