@@ -236,7 +236,7 @@ def run_e2e(args, world, p, hx, hy, hz, n, dev, inb, ref_out):
     import torch
     from gpz_b200.pipeline import SnapshotPipeline
     pipe = SnapshotPipeline(p, n, 3, 32, dev)
-    e2e_steps = max(2, min(args.steps, 6))
+    e2e_steps = max(2, min(args.steps, 10))
     pipe.round_trips([hx, hy, hz], 2)  # warm-up
     barrier(world)
     te0 = time.perf_counter()

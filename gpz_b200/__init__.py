@@ -114,6 +114,7 @@ SIGNATURES = {
     "gpz_decompress": (ctypes.c_int, [_VP, _U64, _U32, _U32, _VP, _VP, _VP, _U64, _VP, _U64,
                                       ctypes.POINTER(Result), _VP]),
     "gpz_result_get": (ctypes.c_int, [_VP, ctypes.POINTER(Result), _VP]),
+    "gpz_result_post": (ctypes.c_int, [_VP, _VP, _VP]),
     "gpz_parse_header": (ctypes.c_int, [_VP, _U64, ctypes.POINTER(_U32), ctypes.POINTER(_U64),
                                         ctypes.POINTER(_U32), ctypes.POINTER(ctypes.c_double),
                                         ctypes.POINTER(_U32)]),
@@ -237,6 +238,16 @@ def result_get(scratch, stream=None) -> Result:
     rc = lib().gpz_result_get(scratch.data_ptr(), ctypes.byref(r), _stream_ptr(stream))
     _check(rc, "gpz_result_get")
     return r
+
+
+def result_post(scratch, host_result, stream=None):
+    """Enqueues a copy of the scratch's result into `host_result`, a pinned
+    uint8 CPU tensor of at least ctypes.sizeof(Result) bytes, without a copy
+    engine; read it with `Result.from_address(host_result.data_ptr())` after
+    the stream has passed this point."""
+    if host_result.device.type != "cpu" or not host_result.is_pinned() or host_result.numel() < ctypes.sizeof(Result):
+        raise GpzError(GPZ_EINVAL, "gpz_result_post")
+    _check(lib().gpz_result_post(scratch.data_ptr(), host_result.data_ptr(), _stream_ptr(stream)), "gpz_result_post")
 
 
 def compress(x, y, z=None, eb: float = 0.0, seg_size: int = 0, rel_mode: bool = False, rel_eb: float = 0.0,

@@ -46,6 +46,15 @@ inline bool aligned16(const void *p) { return ((uintptr_t)p & 15u) == 0; }
 
 inline uint64_t chunks(uint64_t n) { return (n + kChunk - 1) / kChunk; }
 
+// Control-block head (the gpz_result fields) into device-addressable pinned
+// host memory, one word per lane.
+__global__ void result_post_kernel(const gpz_result *src, gpz_result *dst) {
+  constexpr int W = (int)(sizeof(gpz_result) / 4);
+  static_assert(sizeof(gpz_result) % 4 == 0, "word copy");
+  if ((int)threadIdx.x < W)
+    reinterpret_cast<volatile uint32_t *>(dst)[threadIdx.x] = reinterpret_cast<const volatile uint32_t *>(src)[threadIdx.x];
+}
+
 template <typename T>
 int compress_t(const gpz_params *p, const void *d_x, const void *d_y, const void *d_z, void *d_out,
                uint64_t out_capacity, void *d_scratch, uint64_t scratch_bytes, cudaStream_t st) {
@@ -218,6 +227,19 @@ int gpz_result_get(const void *d_scratch, gpz_result *result, void *stream) {
   if (e != cudaSuccess) return GPZ_ECUDA;
   if (result) *result = r;
   return r.status;
+}
+
+int gpz_result_post(const void *d_scratch, gpz_result *h_result, void *stream) {
+  if (!d_scratch || !h_result) return GPZ_EINVAL;
+  cudaPointerAttributes at;
+  if (cudaPointerGetAttributes(&at, h_result) != cudaSuccess) {
+    cudaGetLastError();  // clear the (non-sticky) error the query leaves behind
+    return GPZ_EINVAL;
+  }
+  if (at.type != cudaMemoryTypeHost || at.devicePointer == nullptr) return GPZ_EINVAL;
+  result_post_kernel<<<1, 32, 0, static_cast<cudaStream_t>(stream)>>>(
+      static_cast<const gpz_result *>(d_scratch), static_cast<gpz_result *>(at.devicePointer));
+  return cuda_status(cudaGetLastError());
 }
 
 int gpz_compress(const gpz_params *p, const void *d_x, const void *d_y, const void *d_z, void *d_out,

@@ -10,12 +10,19 @@ encoded or decoded.  Every step still moves its own bytes: the snapshot up,
 the stream down (exactly `stream_bytes`), the stream up again and the
 reconstruction down.
 
-Stages per step i (slot k = i % 2), each on its own stream and ordered by
-events:
+Stages per step i (slot k = i % 2), ordered by events.  All uploads share
+one stream and all downloads another: copies on separate streams of one
+direction are not interleaved by the copy engines (a ready stream copy waited
+behind every queued snapshot upload), so the queue order is set here.  The
+host issues step i's stream download and upload before the next snapshot's
+transfers, and the reconstruction download of step i-1 after the stream
+download of step i, so that each step's dependent chain (down, up,
+decompress) runs ahead of the bulk copies:
 
     upload      host snapshot -> dX[k]            waits: compress of step i-2 done with dX[k]
     compress    dX[k] -> out[k]                    waits: upload; stream download of step i-2
-    size        host reads the stream size         (the one host wait per step)
+    size        host reads the stream size         (the one host wait per step; posted to
+                                                   pinned memory by the device, gpz_result_post)
     down        out[k][:nb] -> pinned hs[k]        waits: compress; stream upload of step i-2
     up          hs[k][:nb] -> din[k]               waits: down; decompress of step i-2
     decompress  din[k] -> oX[k]                    waits: up; reconstruction download of step i-2
@@ -58,10 +65,11 @@ class SnapshotPipeline:
         self.rX = [host_axes() for _ in range(2)]
         self.scr_c = [torch.empty(gz.compress_scratch_bytes(n), dtype=torch.uint8, device=dev) for _ in range(2)]
         self.scr_d = [torch.empty(256, dtype=torch.uint8, device=dev) for _ in range(2)]
+        # compress results land here through gpz_result_post (no copy engine)
+        self.res = [torch.zeros(64, dtype=torch.uint8).pin_memory() for _ in range(2)]
         S = torch.cuda.Stream
-        self.s_up, self.s_up2 = S(device=dev), S(device=dev)
+        self.s_up, self.s_down = S(device=dev), S(device=dev)  # all uploads / all downloads
         self.s_cmp, self.s_dec = S(device=dev), S(device=dev)
-        self.s_down, self.s_fetch = S(device=dev), S(device=dev)
         E = torch.cuda.Event
         names = ("up", "cmp", "down", "up2", "dec", "fetch")
         self.ev = {nm: [E(), E()] for nm in names}
@@ -91,12 +99,15 @@ class SnapshotPipeline:
         d = self.dX[k]
         gz.compress_into(self.p, d[0], d[1], d[2] if self.dim == 3 else d[0], self.out[k], self.scr_c[k],
                          stream=self.s_cmp, sync=False)
+        gz.result_post(self.scr_c[k], self.res[k], stream=self.s_cmp)
         self._record(self.s_cmp, "cmp", k)
 
     def stream_size(self, k: int) -> int:
-        """Waits for the compress of slot k and returns its stream size."""
+        """Waits for the compress of slot k and returns its stream size.  The
+        result was posted to pinned host memory by the device, so this wait
+        does not queue behind the large copies of other steps."""
         self.ev["cmp"][k].synchronize()
-        r = gz.result_get(self.scr_c[k], stream=self.s_cmp)
+        r = gz.Result.from_buffer_copy(self.res[k].numpy().tobytes()[:gz.ctypes.sizeof(gz.Result)])
         if r.status != 0:
             raise gz.GpzError(r.status, "SnapshotPipeline: compress failed")
         self.nb[k] = int(r.stream_bytes)
@@ -114,11 +125,11 @@ class SnapshotPipeline:
     def upload_stream(self, k: int):
         torch = gz._torch()
         nb = self.nb[k]
-        with torch.cuda.stream(self.s_up2):
-            self.s_up2.wait_event(self.ev["down"][k])
-            self._wait(self.s_up2, "dec", k)
+        with torch.cuda.stream(self.s_up):
+            self.s_up.wait_event(self.ev["down"][k])
+            self._wait(self.s_up, "dec", k)
             self.din[k][:nb].copy_(self.hs[k][:nb], non_blocking=True)
-            self._record(self.s_up2, "up2", k)
+            self._record(self.s_up, "up2", k)
 
     def decompress(self, k: int):
         self.s_dec.wait_event(self.ev["up2"][k])
@@ -130,14 +141,14 @@ class SnapshotPipeline:
 
     def fetch(self, k: int):
         torch = gz._torch()
-        with torch.cuda.stream(self.s_fetch):
-            self.s_fetch.wait_event(self.ev["dec"][k])
+        with torch.cuda.stream(self.s_down):
+            self.s_down.wait_event(self.ev["dec"][k])
             for h, d in zip(self.rX[k], self.oX[k]):
                 h.copy_(d, non_blocking=True)
-            self._record(self.s_fetch, "fetch", k)
+            self._record(self.s_down, "fetch", k)
 
     def synchronize(self):
-        for s in (self.s_up, self.s_up2, self.s_cmp, self.s_dec, self.s_down, self.s_fetch):
+        for s in (self.s_up, self.s_cmp, self.s_dec, self.s_down):
             s.synchronize()
 
     # -- the whole schedule ---------------------------------------------------
@@ -150,17 +161,21 @@ class SnapshotPipeline:
             raise gz.GpzError(gz.GPZ_EINVAL, "SnapshotPipeline: steps must be >= 1")
         self.upload(0, host_axes)
         self.compress(0)
+        if steps > 1:
+            self.upload(1, host_axes)
         for i in range(steps):
             k = i & 1
-            if i + 1 < steps:
-                self.upload(k ^ 1, host_axes)  # next snapshot up while this one is encoded
             self.stream_size(k)
             self.download_stream(k)
-            self.upload_stream(k)
+            self.upload_stream(k)  # queued after the upload of snapshot i+1
             self.decompress(k)
-            self.fetch(k)
             if i + 1 < steps:
                 self.compress(k ^ 1)
+            if i >= 1:
+                self.fetch(k ^ 1)  # step i-1's reconstruction, behind step i's stream download
+            if i + 2 < steps:
+                self.upload(k, host_axes)  # snapshot i+2 into the slot compress i has released
+        self.fetch((steps - 1) & 1)
         self.synchronize()
         k = (steps - 1) & 1
         return self.nb[k], self.rX[k]

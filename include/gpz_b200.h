@@ -138,6 +138,16 @@ int gpz_decompress(const void *d_stream, uint64_t stream_bytes, uint32_t float_b
  * (synchronises `stream`). */
 int gpz_result_get(const void *d_scratch, gpz_result *result, void *stream);
 
+/* Enqueues on `stream` a copy of the control block into `h_result`, which must
+ * be pinned host memory the device can address (cudaHostAlloc / cudaMallocHost,
+ * or registered with cudaHostRegister).  A one-thread kernel writes it, so the
+ * copy does not wait behind other transfers on the copy engines; the caller
+ * reads `h_result` once an event recorded after this call has completed.
+ * Returns GPZ_EINVAL for pageable or device memory.  No reference counterpart:
+ * the reference reads its sizes with blocking cudaMemcpy
+ * (src/cudaWarpCompress.cu:1692-1702). */
+int gpz_result_post(const void *d_scratch, gpz_result *h_result, void *stream);
+
 /* ---- helpers -------------------------------------------------------------------- */
 
 /* Host-side header parse of a stream held in host memory.

@@ -39,3 +39,24 @@ def test_round_trips_equal_single_calls(n, dim, bits, steps, abs_eb):
             assert torch.equal(pipe.hs[k][:nb].cuda(), want)
     for h, w in zip(rx, (wx, wy, wz)):
         assert torch.equal(h.view(torch.uint8), w.cpu().view(torch.uint8))
+
+
+@pytest.mark.gpu
+def test_result_post_matches_result_get_and_rejects_pageable_memory():
+    import ctypes
+    import torch
+    n = 50_000
+    x, y, z = (torch.rand(n, device="cuda") * 100 for _ in range(3))
+    p = gz.make_params(n, 3, 32, 0.01, 8)
+    out = torch.empty(gz.stream_bound(n, 3, 32), dtype=torch.uint8, device="cuda")
+    scr = torch.empty(gz.compress_scratch_bytes(n), dtype=torch.uint8, device="cuda")
+    want = gz.compress_into(p, x, y, z, out, scr)
+    host = torch.zeros(64, dtype=torch.uint8).pin_memory()
+    gz.result_post(scr, host)
+    torch.cuda.synchronize()
+    got = gz.Result.from_buffer_copy(host.numpy().tobytes()[:ctypes.sizeof(gz.Result)])
+    assert (got.stream_bytes, got.seg_size, got.status) == (want.stream_bytes, want.seg_size, want.status)
+    pageable = (ctypes.c_uint8 * 64)()
+    assert gz.lib().gpz_result_post(scr.data_ptr(), ctypes.addressof(pageable), None) == gz.GPZ_EINVAL
+    with pytest.raises(gz.GpzError):
+        gz.result_post(scr, torch.zeros(64, dtype=torch.uint8))
