@@ -435,6 +435,14 @@ static __device__ __noinline__ void rank_wide(uint32_t *sw, uint32_t kmin, uint3
   __syncwarp();
 }
 
+// A quantized chunk between the two encode phases: its 31-bit block ids
+// (element j of lane l is point 32j + l), their range, the relative-position
+// bit width and this lane's word of the meta record's min/max part.
+struct ChunkQ {
+  uint32_t key[32];
+  uint32_t kmin, kmax, rbits, mword;
+};
+
 // The points of one chunk, loaded ahead of encoding: float streams keep all
 // axes in registers (element j of lane l is point 32j + l of the chunk), so a
 // chunk costs one round of loads and the next chunk's loads overlap the
@@ -473,12 +481,14 @@ struct ChunkPoints {
   }
 };
 
-// Encodes chunk c into the warp's region `sw`; returns the payload bytes and
-// leaves the meta record in meta[] (word k of the record in lane k).
+// First phase of encoding chunk c: min/max, quantization, block ids (into q)
+// and relative positions (into the warp's third 4 KB, by rank r).  It touches
+// no other part of the warp's region, so it may run while the region's first
+// 8 KB still hold the previous chunk's staged payload.
 template <typename T, int DIM>
-__device__ __forceinline__ uint32_t encode_chunk(const CArgs<T> &a, unsigned long long c, uint32_t *sw,
-                                                 uint32_t seg, uint32_t sh, uint32_t msk, T inv,
-                                                 ChunkPoints<T, DIM> &pts, uint32_t &meta_word, int lane) {
+__device__ __forceinline__ void encode_quantize(const CArgs<T> &a, unsigned long long c, uint32_t *sw,
+                                                uint32_t seg, uint32_t sh, uint32_t msk, T inv,
+                                                ChunkPoints<T, DIM> &pts, ChunkQ &q, int lane) {
   using Tr = TT<T>;
   using UO = typename Tr::U;
   constexpr bool is64 = sizeof(T) == 8;
@@ -488,14 +498,11 @@ __device__ __forceinline__ uint32_t encode_chunk(const CArgs<T> &a, unsigned lon
   const unsigned long long base = c * kChunk;
   const uint32_t nvalid = (uint32_t)min((unsigned long long)kChunk, n - base);
   const bool full = nvalid == (uint32_t)kChunk;
-  // per-warp words: [0,1024) ranked composites -> run starts -> staged payload;
-  // [1024,2048) bucket counts -> deltas -> staged payload; [2048,3072)
-  // relative positions by rank r (staged payload only past 8 KB, after use)
-  uint32_t *const S = sw, *const hist = sw + kChunk, *const relR = sw + 2 * kChunk;
+  uint32_t *const relR = sw + 2 * kChunk;
   const T *const X[3] = {a.x, a.y, a.z};
 
   // ---- 1. quantize one axis at a time (:104-205) ----
-  uint32_t key[32];
+  uint32_t (&key)[32] = q.key;
   T mm[6];
   unsigned long long bnx = 0, bny = 0, bound = 0;
   uint32_t rmax = 0;
@@ -601,10 +608,32 @@ __device__ __forceinline__ uint32_t encode_chunk(const CArgs<T> &a, unsigned lon
     kmin = min(kmin, key[j]);
     kmax = max(kmax, key[j]);
   }
-  kmin = warp_min(kmin);
-  kmax = warp_max(kmax);
+  q.kmin = warp_min(kmin);
+  q.kmax = warp_max(kmax);
   rmax = warp_max(rmax);
-  const uint32_t rbits = max(bitlen(rmax), nvalid < (uint32_t)kChunk ? 1u : 0u);  // :200-201
+  q.rbits = max(bitlen(rmax), nvalid < (uint32_t)kChunk ? 1u : 0u);  // :200-201
+  q.mword = mword;
+}
+
+// Ranks, runs and bit planes of a quantized chunk (encode_quantize left its
+// ids in q and its relative positions in the warp's third 4 KB); stages the
+// payload in the warp's region, returns its bytes and leaves the meta record
+// in meta_word (word k of the record in lane k).
+template <typename T, int DIM>
+__device__ __forceinline__ uint32_t encode_pack(const CArgs<T> &a, unsigned long long c, uint32_t *sw, ChunkQ &q,
+                                                uint32_t &meta_word, int lane) {
+  using Tr = TT<T>;
+  constexpr bool is64 = sizeof(T) == 8;
+  constexpr uint32_t FULL = 0xFFFFFFFFu;
+  const unsigned long long base = c * kChunk;
+  const uint32_t nvalid = (uint32_t)min((unsigned long long)kChunk, a.n - base);
+  const bool full = nvalid == (uint32_t)kChunk;
+  // per-warp words: [0,1024) ranked composites -> run starts -> staged payload;
+  // [1024,2048) bucket counts -> deltas -> staged payload; [2048,3072)
+  // relative positions by rank r (staged payload only past 8 KB, after use)
+  uint32_t *const S = sw, *const hist = sw + kChunk, *const relR = sw + 2 * kChunk;
+  uint32_t (&key)[32] = q.key;
+  const uint32_t kmin = q.kmin, kmax = q.kmax, rbits = q.rbits, mword = q.mword;
 
   // ---- 2. rank the composites (block id - kmin) << 10 | r ----
   const unsigned long long cmax = ((unsigned long long)(kmax - kmin) << 10) | 1023ull;
@@ -793,6 +822,17 @@ __device__ __forceinline__ uint32_t encode_chunk(const CArgs<T> &a, unsigned lon
     meta_word = w;
   }
   return db + cb + rb;
+}
+
+// Encodes chunk c into the warp's region `sw`; returns the payload bytes and
+// leaves the meta record in meta_word (word k of the record in lane k).
+template <typename T, int DIM>
+__device__ __forceinline__ uint32_t encode_chunk(const CArgs<T> &a, unsigned long long c, uint32_t *sw,
+                                                 uint32_t seg, uint32_t sh, uint32_t msk, T inv,
+                                                 ChunkPoints<T, DIM> &pts, uint32_t &meta_word, int lane) {
+  ChunkQ q;
+  encode_quantize<T, DIM>(a, c, sw, seg, sh, msk, inv, pts, q, lane);
+  return encode_pack<T, DIM>(a, c, sw, q, meta_word, lane);
 }
 
 // Copies a staged payload (whole words) to its place in the stream: four

@@ -15,7 +15,7 @@ def test_rejects_bad_shapes_before_allocating():
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("n,dim,bits,steps,abs_eb", [(300_000, 3, 32, 3, 0.0), (70_001, 2, 64, 4, 0.0),
-                                                     (1, 3, 32, 2, 0.01)])
+                                                     (50_000, 3, 64, 1, 0.0), (1, 3, 32, 2, 0.01)])
 def test_round_trips_equal_single_calls(n, dim, bits, steps, abs_eb):
     import torch
     from oracle import pyoracle as po
