@@ -60,3 +60,43 @@ def test_result_post_matches_result_get_and_rejects_pageable_memory():
     assert gz.lib().gpz_result_post(scr.data_ptr(), ctypes.addressof(pageable), None) == gz.GPZ_EINVAL
     with pytest.raises(gz.GpzError):
         gz.result_post(scr, torch.zeros(64, dtype=torch.uint8))
+
+
+STAGES = ["upload", "compress", "stream_size", "download_stream", "upload_stream", "decompress", "fetch"]
+
+
+@pytest.mark.parametrize("steps", [1, 2, 3, 4, 7])
+def test_schedule_orders_stages_and_slot_reuse(steps):
+    """The host schedule, stages stubbed: each step's stages in dependency
+    order, each once, and a slot refilled only after the previous step on
+    that slot has issued the stage that reads it (the event every wait names
+    must already be recorded when the wait is enqueued)."""
+    pipe = object.__new__(SnapshotPipeline)
+    log = []
+    for name in STAGES:
+        setattr(pipe, name, (lambda nm: lambda k, *a: log.append((nm, k)))(name))
+    pipe.synchronize = lambda: log.append(("sync", -1))
+    pipe.nb, pipe.rX = [0, 0], [[], []]
+    pipe.round_trips([None], steps)
+    assert log[-1] == ("sync", -1)
+    seen, pos = {}, {}
+    for idx, (nm, k) in enumerate(log[:-1]):
+        j = seen.get((nm, k), 0)
+        seen[(nm, k)] = j + 1
+        pos[(nm, 2 * j + k)] = idx  # the j-th use of slot k is step 2j + k
+    assert sorted(pos) == sorted((nm, i) for nm in STAGES for i in range(steps))
+    for i in range(steps):
+        for a, b in zip(STAGES, STAGES[1:]):
+            assert pos[(a, i)] < pos[(b, i)], (i, a, b)
+    for i in range(2, steps):
+        assert pos[("compress", i - 2)] < pos[("upload", i)]
+        assert pos[("download_stream", i - 2)] < pos[("compress", i)]
+        assert pos[("upload_stream", i - 2)] < pos[("download_stream", i)]
+        assert pos[("decompress", i - 2)] < pos[("upload_stream", i)]
+        assert pos[("fetch", i - 2)] < pos[("decompress", i)]
+
+
+def test_schedule_rejects_zero_steps():
+    pipe = object.__new__(SnapshotPipeline)
+    with pytest.raises(gz.GpzError):
+        pipe.round_trips([None], 0)
