@@ -477,6 +477,18 @@ struct ChunkPoints {
             v[d][j] = X[d][base + (p < nvalid ? p : 0u)];
           }
       }
+    } else {
+      // Double streams keep no points in registers: lane d asks for axis d
+      // of the chunk in L2 (one bulk prefetch of its valid, 16-byte aligned
+      // span), so that the quantize phase's loads hit L2.
+      if (lane < DIM && c < a.G) {
+        const unsigned long long base = c * kChunk;
+        const uint32_t nvalid = (uint32_t)min((unsigned long long)kChunk, a.n - base);
+        const T *p = (lane == 0 ? a.x : (lane == 1 ? a.y : a.z)) + base;
+        const uint32_t bytes = (nvalid * (uint32_t)sizeof(T)) & ~15u;
+        if (bytes != 0u && (reinterpret_cast<uintptr_t>(p) & 15u) == 0u)
+          asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
+      }
     }
   }
 };
