@@ -61,6 +61,8 @@ def test_host_argument_errors_without_gpu():
     assert rc == gz.GPZ_EINVAL
     rc = lib.gpz_decompress_async(16, 100, 16, 3, 16, 16, 16, 10, 256, 256, None)
     assert rc == gz.GPZ_EINVAL
+    assert lib.gpz_result_post(None, 16, None) == gz.GPZ_EINVAL  # no scratch
+    assert lib.gpz_result_post(16, None, None) == gz.GPZ_EINVAL  # no host result
 
 
 @pytest.mark.parametrize("check", ["fastdiv_check", "transpose_check", "network_check"])
