@@ -67,6 +67,14 @@ def traffic_from_profile(n):
     return None
 
 
+def bench_config(n, world, seg, sbytes):
+    """The `config` object of the JSON line (both arms print the same keys)."""
+    return {"workload": WORKLOAD, "points_per_gpu": n, "dim": 3, "error_mode": "rel", "error_bound": REL_EB,
+            "segment_size": int(seg), "stream_bytes": int(sbytes), "compression_ratio": round(n * 12 / sbytes, 4),
+            "parallelism": f"{world} independent snapshots",
+            "l2": "inputs (1.72 GB per GPU) larger than the 126 MB L2; no flush"}
+
+
 def gen_clustered(n, seed, device):
     """Synthetic stand-in for the SDRBench/HACC-style snapshot (not in this container)."""
     import torch
@@ -194,7 +202,76 @@ def cpu_baseline_run(x, y, z, steps=1):
         s = po.compress(x, y, z, 3, eb, seg, nthreads=cores)
         po.decompress(s, nthreads=cores)
         ts.append(time.perf_counter() - t0)
-    return ts, cores, len(s)
+    return ts, cores, len(s), seg
+
+
+REF_BUILDS = (("gpz_ref_sm100a", "reference sources built for sm_100a"),
+              ("gpz_ref_ptx90", "stock CMake architectures (compute_90 PTX, JIT-compiled on the B200)"))
+
+
+def reference_gpu_run(hx, hy, hz, n, eb, rel, ours_stream, ours_rec, reps):
+    """Times the reference's own GPU codec on the same snapshot, in this run.
+
+    The reference is built from its sources by oracle/Makefile (target `ref`)
+    into oracle/_ref/; its harness (oracle/ref_harness.cu) drives the
+    reference's CompressorManager with the CLI's scratch and buffer sizes and
+    times compressWarp / decompressWarp with CUDA events, the scope of the
+    reference CLI's own timer (src/main.cpp:336-346).  The first repetition
+    (PTX JIT, first-touch) is dropped.  Its stream and reconstruction are
+    compared byte for byte with this codec's."""
+    import numpy as np
+    out = {}
+    exes = {b: os.path.join(ROOT, "oracle", "_ref", b) for b, _ in REF_BUILDS}
+    if not any(os.path.exists(e) for e in exes.values()):
+        return {"unavailable": "reference build oracle/_ref/ not present (make -C oracle ref)"}
+    tmp = tempfile.mkdtemp(prefix="gpz_refgpu_")
+    soa = os.path.join(tmp, "in.soa")
+    with open(soa, "wb") as f:
+        for a in (hx, hy, hz):
+            f.write(memoryview(a.numpy()).cast("B"))
+    inb = n * 12
+    try:
+        for b, what in REF_BUILDS:
+            exe = exes[b]
+            if not os.path.exists(exe):
+                out[b] = {"unavailable": "not built"}
+                continue
+            st, rec = os.path.join(tmp, "ref.gpz"), os.path.join(tmp, "ref.rec")
+            p = subprocess.run([exe, "compress", soa, str(n), "3", "32", repr(eb), repr(rel), "rel", "0", st,
+                                str(reps + 1)], capture_output=True, text=True)
+            if p.returncode != 0:
+                out[b] = {"unavailable": "compress failed: " + (p.stdout + p.stderr).strip()[-200:]}
+                continue
+            c = json.loads(p.stdout.strip().splitlines()[-1])
+            cms = c["ms"][1:] or c["ms"]
+            d = subprocess.run([exe, "decompress", st, rec, str(reps + 1)], capture_output=True, text=True)
+            rs = np.fromfile(st, np.uint8)
+            line = {"build": what, "compress_ms_best": round(min(cms), 4),
+                    "compress_ms_median": round(statistics.median(cms), 4),
+                    "compress_gbs_best": round(inb / min(cms) / 1e6, 2), "stream_bytes": int(c["bytes"]),
+                    "segment_size": int(c["seg"]),
+                    "identical_stream": bool(rs.size == ours_stream.size and np.array_equal(rs, ours_stream))}
+            del rs
+            if d.returncode == 0:
+                dj = json.loads(d.stdout.strip().splitlines()[-1])
+                dms = dj["ms"][1:] or dj["ms"]
+                rr = np.fromfile(rec, np.uint8)
+                line.update(decompress_ms_best=round(min(dms), 4), decompress_ms_median=round(statistics.median(dms), 4),
+                            decompress_gbs_best=round(inb / min(dms) / 1e6, 2),
+                            identical_reconstruction=bool(rr.size == ours_rec.size and np.array_equal(rr, ours_rec)))
+                del rr
+            else:
+                line["decompress"] = "not run: " + (d.stdout + d.stderr).strip()[-200:]
+            line["reps"] = len(cms)
+            out[b] = line
+            for q in (st, rec):
+                if os.path.exists(q):
+                    os.remove(q)
+    finally:
+        if os.path.exists(soa):
+            os.remove(soa)
+        os.rmdir(tmp)
+    return out
 
 
 def run_reference(args):
@@ -209,14 +286,14 @@ def run_reference(args):
     x, y, z = (t.cpu().numpy() for t in gen_clustered(N_POINTS, 1234, dev))
     if args.warmup > 0:
         cpu_baseline_run(x, y, z, args.warmup)
-    ts, cores, sbytes = cpu_baseline_run(x, y, z, args.steps)
+    ts, cores, sbytes, seg = cpu_baseline_run(x, y, z, args.steps)
     step = sum(ts) / len(ts)
     val = N_POINTS * 12 / step / 1e9
     line = {
         "impl": "reference", "metric": METRIC, "value": round(val, 4), "unit": "GB/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(step * 1e3, 3), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "points": N_POINTS, "dim": 3, "error_mode": "rel", "error_bound": REL_EB},
+        "config": bench_config(N_POINTS, world, seg, sbytes),
         "cpu_baseline": {"value": round(val, 4), "unit": "GB/s", "cores": cores, "kind": "port",
                          "sample": f"the full snapshot ({N_POINTS} points) per step, compress + decompress, "
                                    "OpenMP C++ restatement of the reference algorithm (the reference has no "
@@ -278,6 +355,8 @@ def run_ours(args):
     hdr = gz.parse_header(out[:32].cpu().numpy().tobytes())
     ver = gz.verify(x, y, z, ox, oy, oz, hdr["eb"], hdr["seg"])
     assert ver.over_bound_tol == 0, ver.over_bound_tol  # the reference verifier's 1.01*eb tolerance
+    ref_stream = out[:sbytes].clone()
+    ref_rec = [t.clone() for t in (ox, oy, oz)]
 
     def step(evs=None):
         if evs is not None:
@@ -303,6 +382,14 @@ def run_ours(args):
         t1.record(stream)
         torch.cuda.synchronize()
     barrier(world)
+    # the timed launches did the work: both calls of the last step report
+    # success, and its stream and reconstruction equal the verified ones
+    rc_, rd_ = gz.result_get(scr_c, stream), gz.result_get(scr_d, stream)
+    if rc_.status != 0 or rd_.status != 0 or int(rc_.stream_bytes) != sbytes:
+        raise RuntimeError(f"timed launches failed: compress {rc_.status}, decompress {rd_.status}")
+    if not torch.equal(out[:sbytes], ref_stream) or not all(torch.equal(a, b) for a, b in zip((ox, oy, oz), ref_rec)):
+        raise RuntimeError("timed launches produced a different stream or reconstruction")
+    del ref_rec
     total_ms = max_over_ranks(t0.elapsed_time(t1), world)
     c_ms = [e[0].elapsed_time(e[1]) for e in evs]
     d_ms = [e[1].elapsed_time(e[2]) for e in evs]
@@ -326,9 +413,17 @@ def run_ours(args):
     else:
         e2e_val, nb, e2e_steps = run_e2e(args, world, p, hx, hy, hz, n, dev, inb, (ox, oy, oz))
 
+    ref_gpu = None
+    if world == 1 and rank == 0 and not args.no_reference_gpu:
+        import numpy as np
+        ours_stream = out[:sbytes].cpu().numpy()
+        ours_rec = np.concatenate([t.cpu().numpy() for t in (ox, oy, oz)]).view(np.uint8)
+        ref_gpu = reference_gpu_run(hx, hy, hz, n, float(eb), rel, ours_stream, ours_rec, max(3, min(args.steps, 10)))
+        del ours_stream, ours_rec
+
     cpu = None
     if world == 1 and rank == 0 and not args.no_cpu_baseline:
-        ts, cores, _ = cpu_baseline_run(hx.numpy(), hy.numpy(), hz.numpy(), 1)
+        ts, cores, _, _ = cpu_baseline_run(hx.numpy(), hy.numpy(), hz.numpy(), 1)
         cpu = {"value": round(inb / ts[0] / 1e9, 4), "unit": "GB/s", "cores": cores, "kind": "port",
                "sample": f"one compress + decompress of the same {n}-point snapshot on {cores} host threads "
                          "(OpenMP C++ restatement of the reference algorithm)"}
@@ -339,10 +434,7 @@ def run_ours(args):
             "warmup": max(args.warmup, 3), "ms_per_step": round(ms_step, 4), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (seeded clustered generator standing in for SDRBench HACC-style snapshots)",
-            "config": {"workload": WORKLOAD, "points_per_gpu": n, "dim": 3, "error_mode": "rel",
-                       "error_bound": REL_EB, "segment_size": int(r.seg_size), "stream_bytes": sbytes,
-                       "compression_ratio": round(inb / sbytes, 4), "parallelism": f"{world} independent snapshots",
-                       "l2": "inputs (1.72 GB per GPU) larger than the 126 MB L2; no flush"},
+            "config": bench_config(n, world, r.seg_size, sbytes),
             "verified": {"points": int(ver.points), "over_bound": int(ver.over_bound),
                          "over_1.01eb": int(ver.over_bound_tol),
                          "max_abs_err": [round(v, 9) for v in ver.max_abs_err], "eb": hdr["eb"],
@@ -359,6 +451,7 @@ def run_ours(args):
                    {"value": round(e2e_val, 4), "unit": "GB/s", "h2d_bytes_per_step": inb + nb,
                     "d2h_bytes_per_step": nb + inb, "steps": e2e_steps},
             "cpu_baseline": cpu,
+            "reference_gpu": ref_gpu,
         }
         print(json.dumps(line), flush=True)
     if world > 1:
@@ -663,6 +756,8 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer end-to-end timing")
+    ap.add_argument("--no-reference-gpu", action="store_true",
+                    help="skip timing the reference's own GPU build on the same snapshot")
     ap.add_argument("--batched", action="store_true",
                     help="time the batched form (many snapshots per graph launch) against per-snapshot calls")
     ap.add_argument("--batch", type=int, default=256, help="snapshots in the batched workload")

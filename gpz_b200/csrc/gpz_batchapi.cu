@@ -19,6 +19,7 @@
 #include "gpz_b200.h"
 #include "gpz_batch.cuh"
 #include "gpz_batch_host.h"
+#include "gpz_launch.h"
 
 using namespace gpzb;
 
@@ -86,37 +87,19 @@ __global__ void __launch_bounds__(256) batch_rel_mapped_kernel(BItem<T> *items, 
   rel_to_abs_block<T>(it.a.x, it.a.y, it.a.z, it.a.n, it.a.dim, it.rel_eb, it.rctl, &it.a.eb, b, nb);
 }
 
-int num_sms_now() {
-  int dev = 0, sms = 148;
-  if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  return sms > 0 ? sms : 148;
-}
-
-// CTAs per SM of a kernel with `smem` dynamic shared memory (the attribute is
-// set once per kernel and process; 0 when the query fails).
-template <typename K>
-int resident_ctas(K kernel, int threads, size_t smem, int &cache) {
-  if (cache) return cache;
-  if (cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) return 0;
-  int occ = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kernel, threads, smem) != cudaSuccess || occ < 1) occ = 1;
-  cache = occ;
-  return occ;
-}
-
+// Grids of the batched persistent kernels on the current device (-1 when the
+// kernel's shared-memory attribute cannot be raised there).
 template <typename T, int DIM>
 int compress_grid(uint64_t groups) {
-  static int occ = 0;
-  const int o = resident_ctas(compress_batch_kernel<T, DIM>, 32 * kEncWarps, enc_smem_bytes(), occ);
-  return o ? (int)std::min<uint64_t>(groups, (uint64_t)num_sms_now() * o) : -1;
+  const int o = resident_ctas(compress_batch_kernel<T, DIM>, 32 * kEncWarps, enc_smem_bytes());
+  return o ? (int)std::min<uint64_t>(groups, (uint64_t)current_sms() * o) : -1;
 }
 
 template <typename T, int DIM>
 int dec_grid(uint64_t chunks) {
-  static int occ = 0;
   constexpr int W = DecCfg<T>::warps;
-  const int o = resident_ctas(decompress_batch_kernel<T, DIM>, 32 * W, dec_smem_bytes<T>(), occ);
-  return o ? (int)std::min<uint64_t>((chunks + W - 1) / W, (uint64_t)num_sms_now() * o) : -1;
+  const int o = resident_ctas(decompress_batch_kernel<T, DIM>, 32 * W, dec_smem_bytes<T>());
+  return o ? (int)std::min<uint64_t>((chunks + W - 1) / W, (uint64_t)current_sms() * o) : -1;
 }
 
 template <typename T, int DIM>

@@ -12,7 +12,10 @@
 #include <cstring>
 #include <mutex>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include "gpz_b200.h"
+#include "gpz_launch.h"
 #include "gpz_kernels.cuh"
 #include "gpz_encode.cuh"
 #include "gpz_decode.cuh"
@@ -21,26 +24,19 @@ using namespace gpzb;
 
 namespace {
 
-int g_num_sms = 0;
-
-int num_sms() {
-  if (g_num_sms == 0) {
-    int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess) return 148;
-    if (cudaDeviceGetAttribute(&g_num_sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) g_num_sms = 148;
-  }
-  return g_num_sms;
-}
-
-template <typename K>
-int occupancy(K kernel, int threads = kThreads) {
-  int blocks = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, kernel, threads, 0) != cudaSuccess || blocks < 1)
-    blocks = 1;
-  return blocks;
-}
+int num_sms() { return current_sms(); }
 
 inline int cuda_status(cudaError_t e) { return e == cudaSuccess ? GPZ_OK : GPZ_ECUDA; }
+
+// NVTX range for the duration of a scope, with the names the reference's
+// codec pushes (src/cudaWarpCompress.cu:1577, 1626, 1747, 1817), so profiler
+// timelines of either codec line up.
+struct NvtxRange {
+  explicit NvtxRange(const char *name) { nvtxRangePushA(name); }
+  ~NvtxRange() { nvtxRangePop(); }
+  NvtxRange(const NvtxRange &) = delete;
+  NvtxRange &operator=(const NvtxRange &) = delete;
+};
 
 inline bool aligned16(const void *p) { return ((uintptr_t)p & 15u) == 0; }
 
@@ -59,6 +55,7 @@ template <typename T>
 int compress_t(const gpz_params *p, const void *d_x, const void *d_y, const void *d_z, void *d_out,
                uint64_t out_capacity, void *d_scratch, uint64_t scratch_bytes, cudaStream_t st) {
   using Tr = TT<T>;
+  NvtxRange range("compress");
   const uint64_t G = chunks(p->n);
   if (out_capacity < Tr::hdr + G * (8ull + Tr::meta)) return GPZ_ENOSPACE;
   if (scratch_bytes < gpz_compress_scratch_bytes(p->n)) return GPZ_ENOSPACE;
@@ -89,26 +86,22 @@ int compress_t(const gpz_params *p, const void *d_x, const void *d_y, const void
   a.vec_ok = aligned16(d_x) && aligned16(d_y) && (p->dim == 2 || aligned16(d_z));
   // persistent grid: one CTA per kEncWarps chunks in flight
   constexpr size_t smem = enc_smem_bytes();
-  auto launch = [&](auto kernel, int &occ) -> cudaError_t {
-    if (!occ) {
-      cudaError_t e2 = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-      if (e2 != cudaSuccess) return e2;
-      if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kernel, 32 * kEncWarps, smem) != cudaSuccess || occ < 1)
-        occ = 1;
-    }
+  NvtxRange krange("run compress kernel");
+  auto launch = [&](auto kernel) -> bool {
+    const int occ = resident_ctas(kernel, 32 * kEncWarps, smem);
+    if (occ == 0) return false;
     const uint64_t grid = std::min<uint64_t>((G + kEncWarps - 1) / kEncWarps, (uint64_t)num_sms() * occ);
     kernel<<<(unsigned)grid, 32 * kEncWarps, smem, st>>>(a);
-    return cudaSuccess;
+    return true;
   };
-  static int occ3 = 0, occ2 = 0;
-  e = p->dim == 3 ? launch(compress_kernel<T, 3>, occ3) : launch(compress_kernel<T, 2>, occ2);
-  if (e != cudaSuccess) return GPZ_ECUDA;
+  if (!(p->dim == 3 ? launch(compress_kernel<T, 3>) : launch(compress_kernel<T, 2>))) return GPZ_ECUDA;
   return cuda_status(cudaGetLastError());
 }
 
 template <typename T>
 int decompress_t(const void *d_stream, uint64_t stream_bytes, uint32_t dim, void *d_x, void *d_y, void *d_z,
                  uint64_t out_capacity, void *d_scratch, uint64_t scratch_bytes, cudaStream_t st) {
+  NvtxRange range("decompress");
   if (scratch_bytes < gpz_decompress_scratch_bytes()) return GPZ_ENOSPACE;
   if (((uintptr_t)d_stream & 7u) != 0) return GPZ_EINVAL;
   Control *ctl = static_cast<Control *>(d_scratch);
@@ -128,19 +121,15 @@ int decompress_t(const void *d_stream, uint64_t stream_bytes, uint32_t dim, void
   constexpr int W = DecCfg<T>::warps;
   constexpr size_t smem = dec_smem_bytes<T>();
   const uint64_t bound_ctas = (stream_bytes / (8ull + TT<T>::meta) + W) / W;
-  auto launch = [&](auto kernel, int &occ) -> cudaError_t {
-    if (!occ) {
-      cudaError_t e2 = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-      if (e2 != cudaSuccess) return e2;
-      if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kernel, 32 * W, smem) != cudaSuccess || occ < 1) occ = 1;
-    }
+  NvtxRange krange("run decompress kernel");
+  auto launch = [&](auto kernel) -> bool {
+    const int occ = resident_ctas(kernel, 32 * W, smem);
+    if (occ == 0) return false;
     const uint64_t grid = std::min<uint64_t>((uint64_t)num_sms() * occ, bound_ctas);
     kernel<<<(unsigned)grid, 32 * W, smem, st>>>(a);
-    return cudaSuccess;
+    return true;
   };
-  static int occ3 = 0, occ2 = 0;
-  e = dim == 3 ? launch(decompress_kernel<T, 3>, occ3) : launch(decompress_kernel<T, 2>, occ2);
-  if (e != cudaSuccess) return GPZ_ECUDA;
+  if (!(dim == 3 ? launch(decompress_kernel<T, 3>) : launch(decompress_kernel<T, 2>))) return GPZ_ECUDA;
   return cuda_status(cudaGetLastError());
 }
 

@@ -38,6 +38,9 @@ struct DArgs {
 //   P   per-position id (fast path: then running quotients) or run index
 //   R   per-position relative position word
 //   C   staged output rows
+#ifndef GPZ_DEC_MIN_CTAS_F32
+#define GPZ_DEC_MIN_CTAS_F32 4  // resident float32 decoder CTAs per SM the register budget is sized for
+#endif
 template <typename T> struct DecCfg;
 template <> struct DecCfg<float> {
   static constexpr int warps = 4, min_ctas = GPZ_DEC_MIN_CTAS_F32;

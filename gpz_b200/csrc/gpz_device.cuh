@@ -2,10 +2,10 @@
 //
 // Layout and arithmetic follow the GPZ reference format (path:line citations
 // refer to the reference project); the parallel decomposition is this
-// library's own: one 256-thread CTA per 1024-point chunk in a persistent grid,
-// bucketed composite-key ranking instead of a radix sort, in-register bit
+// library's own: one warp per 1024-point chunk in persistent grids, register
+// sorting networks for the stable order by block id, in-register bit
 // transposes for the bit planes, and a single-pass decoupled look-back scan
-// that places each chunk's payload directly in the output stream.
+// that places each group's payloads directly in the output stream.
 #pragma once
 
 #include <cstdint>
@@ -15,22 +15,9 @@
 namespace gpzb {
 
 constexpr int kChunk = 1024;        // points per chunk (ELEMS_PER_BLOCK, include/cudaCompress.cuh:9-11)
-constexpr int kThreads = 256;       // threads per CTA
-constexpr int kWarps = kThreads / 32;
-constexpr int kEPT = kChunk / kThreads;   // points per thread (4)
-constexpr int kBucketBits = 12;     // ranking buckets per chunk: 4096
-constexpr int kBuckets = 1 << kBucketBits;
-constexpr int kSmallBucket = 16;    // larger ranking buckets are sorted by a warp
 constexpr int kStageBytes = 9472;   // >= max payload: 31*128 + 11*128 + 31*128 + padding
 constexpr uint32_t kSpinLimit = 1u << 22;  // bounded waits in the look-back scan
 constexpr int kCtlBytes = 256;      // control block at the head of scratch
-#ifndef GPZ_COMPRESS_MIN_BLOCKS
-#define GPZ_COMPRESS_MIN_BLOCKS 4
-#endif
-#ifndef GPZ_DEC_MIN_CTAS_F32
-#define GPZ_DEC_MIN_CTAS_F32 4
-#endif
-constexpr int kCompressMinBlocks = GPZ_COMPRESS_MIN_BLOCKS;  // resident CTAs per SM the register budget is sized for
 
 // Error codes (same values as include/gpz_b200.h).
 constexpr int kOK = 0, kEINVAL = 1, kESEG = 2, kESTREAM = 3, kENOSPACE = 4, kETIMEOUT = 6;

@@ -282,22 +282,49 @@ struct gpz_server {
     uint8_t *img = s.image;
     const Clock::time_point now = Clock::now();
     for (uint64_t t : chosen) reqs[t].t_launch = now;
+    // every enqueue is checked: a batch whose upload, launch or status
+    // read-back could not be queued is failed as a whole (GPZ_ECUDA) instead
+    // of being retired later with stale status bytes
+    bool queued = true;
+    auto ck = [&](cudaError_t e) { queued &= e == cudaSuccess; };
     if (!ci.empty()) {
       gpzb_host::compress_tables(ci.data(), Lc, ws, img);
-      cudaMemcpyAsync(ws + Lc.zero_bytes, img, Lc.bytes - Lc.zero_bytes, cudaMemcpyHostToDevice, s.st);
-      gpzb_host::compress_enqueue(Lc, ws, s.st);
+      ck(cudaMemcpyAsync(ws + Lc.zero_bytes, img, Lc.bytes - Lc.zero_bytes, cudaMemcpyHostToDevice, s.st));
+      if (queued) gpzb_host::compress_enqueue(Lc, ws, s.st);
+      ck(cudaGetLastError());
       img += up(Lc.bytes - Lc.zero_bytes);
     }
-    if (!di.empty()) {
+    if (queued && !di.empty()) {
       gpzb_host::decompress_tables(di.data(), Ld, wsd, img);
-      cudaMemcpyAsync(wsd + Ld.zero_bytes, img, Ld.bytes - Ld.zero_bytes, cudaMemcpyHostToDevice, s.st);
-      gpzb_host::decompress_enqueue(Ld, wsd, s.st);
+      ck(cudaMemcpyAsync(wsd + Ld.zero_bytes, img, Ld.bytes - Ld.zero_bytes, cudaMemcpyHostToDevice, s.st));
+      if (queued) gpzb_host::decompress_enqueue(Ld, wsd, s.st);
+      ck(cudaGetLastError());
     }
     const uint64_t nc = ci.size();
-    if (nc) cudaMemcpyAsync(s.ctl_h, ws, 2 * nc * kCtlBytes, cudaMemcpyDeviceToHost, s.st);
-    if (!di.empty())
-      cudaMemcpyAsync(s.ctl_h + 2 * nc * kCtlBytes, wsd, di.size() * kCtlBytes, cudaMemcpyDeviceToHost, s.st);
-    cudaEventRecord(s.done, s.st);
+    if (queued && nc) ck(cudaMemcpyAsync(s.ctl_h, ws, 2 * nc * kCtlBytes, cudaMemcpyDeviceToHost, s.st));
+    if (queued && !di.empty())
+      ck(cudaMemcpyAsync(s.ctl_h + 2 * nc * kCtlBytes, wsd, di.size() * kCtlBytes, cudaMemcpyDeviceToHost, s.st));
+    if (queued) ck(cudaEventRecord(s.done, s.st));
+    if (!queued) {
+      // wait out whatever part of the batch did get queued (its kernels use
+      // the slot's workspace), then complete its requests with the error
+      cudaStreamSynchronize(s.st);
+      cudaGetLastError();
+      const Clock::time_point t_end = Clock::now();
+      for (uint64_t t : chosen) {
+        Req &q = reqs[t];
+        q.c.status = GPZ_ECUDA;
+        q.c.queue_ms = ms_between(q.t_submit, q.t_launch);
+        q.c.total_ms = ms_between(q.t_submit, t_end);
+        q.c.batch_size = (uint32_t)chosen.size();
+        q.done = true;
+        ++completed;
+      }
+      s.comp.clear();
+      s.dec.clear();
+      cv_done.notify_all();
+      return true;
+    }
     last = s.done;
     s.busy = true;
     ++batches;

@@ -21,6 +21,7 @@
 
 #include "gpz_b200.h"
 #include "gpz_kernels.cuh"
+#include "gpz_launch.h"
 
 using namespace gpzb;
 
@@ -186,17 +187,16 @@ int verify_t(uint32_t dim, uint64_t n, const void *dx, const void *dy, const voi
   const size_t smem = (size_t)kVerifyWarps * kChunk * 8;
   const T *x = (const T *)dx, *y = (const T *)dy, *z = (const T *)(dim == 3 ? dz : dy);
   const T *a = (const T *)rx, *b = (const T *)ry, *c = (const T *)(dim == 3 ? rz : ry);
-  int sms = 148, dev = 0;
-  cudaGetDevice(&dev);
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const int sms = current_sms();
   const uint64_t G = (n + kChunk - 1) / kChunk;
-  auto launch = [&](auto kernel) {
-    cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    const uint64_t grid = std::min<uint64_t>((G + kVerifyWarps - 1) / kVerifyWarps, (uint64_t)sms * 3);
+  auto launch = [&](auto kernel) -> bool {
+    const int occ = resident_ctas(kernel, 32 * kVerifyWarps, smem);
+    if (occ == 0) return false;
+    const uint64_t grid = std::min<uint64_t>((G + kVerifyWarps - 1) / kVerifyWarps, (uint64_t)sms * occ);
     kernel<<<(unsigned)grid, 32 * kVerifyWarps, smem, st>>>(x, y, z, a, b, c, n, (T)eb, seg, acc);
+    return true;
   };
-  if (dim == 3) launch(verify_kernel<T, 3>);
-  else launch(verify_kernel<T, 2>);
+  if (!(dim == 3 ? launch(verify_kernel<T, 3>) : launch(verify_kernel<T, 2>))) return GPZ_ECUDA;
   if (cudaGetLastError() != cudaSuccess) return GPZ_ECUDA;
   VerifyAcc h;
   if (cudaMemcpyAsync(&h, acc, sizeof(h), cudaMemcpyDeviceToHost, st) != cudaSuccess) return GPZ_ECUDA;

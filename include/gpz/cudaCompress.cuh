@@ -1,7 +1,7 @@
 // cudaCompress.cuh -- CudaConfig, as declared by the GPZ reference
 // (include/cudaCompress.cuh:16-40): same fields, constructors and meaning, so
 // code written against the reference compiles unchanged.  Implemented by the
-// B200 library (gpz_b200/csrc/gpz_plugin.cpp) on top of include/gpz_b200.h.
+// B200 library (gpz_b200/csrc/gpz_plugin.cu) on top of include/gpz_b200.h.
 #ifndef GPZ_B200_CUDA_COMPRESS_H
 #define GPZ_B200_CUDA_COMPRESS_H
 

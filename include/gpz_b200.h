@@ -180,11 +180,13 @@ int gpz_rel_to_abs(uint32_t float_bits, uint32_t dim, uint64_t n, const void *d_
  *
  * Limit: n <= gpz_compress_noalloc_max_points() (536,838,144 points);
  * larger inputs return GPZ_ELIMIT before anything is launched.
- * The first call on each device looks up the array's device address
- * (cudaGetSymbolAddress); make that first call before any stream capture.
+ * The first call on each device also looks up the array's device address
+ * (cudaGetSymbolAddress), so make that first call before any stream capture
+ * begins.  Every call, the first included, waits for `stream` to finish,
+ * because it reads the result back to the host.
  * All calls share the one array: calls that overlap on the GPU (different
  * streams, or different host threads on the same device) race and must be
- * serialised by the caller.  Synchronises `stream` to return the result. */
+ * serialised by the caller. */
 uint64_t gpz_compress_noalloc_max_points(void);
 int gpz_compress_noalloc(const gpz_params *params, const void *d_x, const void *d_y,
                          const void *d_z, void *d_out, uint64_t out_capacity,

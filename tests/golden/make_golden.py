@@ -13,10 +13,17 @@ by the oracle's generators, and records:
 * one run of the reference CLI (src/main.cpp) to pin the relative-bound
   conversion it performs on the host.
 
-Needs a GPU (run on the B200 box):
-    make -C oracle && make -C oracle ref    # here, once
-    python tests/golden/make_golden.py --out gpurun_out/golden
-then copy gpurun_out/golden/* into tests/golden/.
+With ``--full`` it instead records, for the full-size workloads (FULL below:
+the 143,735,721-point clustered float32 snapshot at rel 1e-4 and at abs 1e-3
+with segment size 32, the 200,000,000-point float64 FCC lattice and the
+100,000,000-point float64 2D square lattice at rel 1e-5), the SHA-256 of the
+reference's stream and, where its decoder can run, of its reconstruction, in
+``full_size.json``.
+
+Needs a GPU:
+    make -C oracle && make -C oracle ref    # once, where the reference sources are
+    python tests/golden/make_golden.py --out <dir> [--full]
+then copy <dir>/* into tests/golden/.
 """
 from __future__ import annotations
 
@@ -66,6 +73,90 @@ CASES = [
 ]
 
 
+# name, workload, n, dim, bits, mode, e, seg
+FULL = [
+    ("clustered_f32_143M_rel1e-4", "clustered", 143_735_721, 3, 32, "rel", 1e-4, 0),
+    ("clustered_f32_143M_abs1e-3_s32", "clustered", 143_735_721, 3, 32, "abs", 1e-3, 32),
+    ("fcc_f64_200M_rel1e-5", "fcc", 200_000_000, 3, 64, "rel", 1e-5, 0),
+    ("square_f64_100M_rel1e-5", "square", 100_000_000, 2, 64, "rel", 1e-5, 0),
+]
+
+
+def full_input(workload, n):
+    """Host SoA arrays (x, y, z) of a full-size workload; z is zeros in 2D.
+
+    clustered: the bench generator (70 % in 20,000 Gaussian clusters, 30 %
+    uniform, box [0,1000)^3, shuffled; seed 1234), drawn on cuda:0.
+    fcc / square: the oracle's lattice generator (spacing 1, Gaussian jitter
+    sigma 0.05, random order; seed 2024)."""
+    if workload == "clustered":
+        import bench
+        return tuple(t.cpu().numpy() for t in bench.gen_clustered(n, 1234, "cuda"))
+    dim = 3 if workload == "fcc" else 2
+    return po.generate(2, n, dim, 0.0, 0.05, 2024, np.float64)
+
+
+def full_eb(x, y, z, dim, bits, mode, e):
+    """The absolute bound the reference CLI passes to the codec."""
+    if mode != "rel":
+        return float(np.float32(e)) if bits == 32 else float(e)
+    return po.rel_to_abs(x, y, z if dim == 3 else None, e)
+
+
+def sha_array(*arrays) -> str:
+    h = hashlib.sha256()
+    for a in arrays:
+        h.update(memoryview(np.ascontiguousarray(a)).cast("B"))
+    return h.hexdigest()
+
+
+def main_full(args):
+    tmp = tempfile.mkdtemp(prefix="gpz_golden_full_")
+    recs = []
+    for (name, workload, n, dim, bits, mode, e, seg) in FULL:
+        x, y, z = full_input(workload, n)
+        eb = full_eb(x, y, z, dim, bits, mode, e)
+        soa = os.path.join(tmp, "in.soa")
+        with open(soa, "wb") as f:
+            for a in (x, y, z):
+                f.write(memoryview(np.ascontiguousarray(a)).cast("B"))
+        del x, y, z
+        sfile = os.path.join(tmp, "out.gpz")
+        rc, out, err = run([HARNESS, "compress", soa, str(n), str(dim), str(bits), repr(eb), repr(e), mode,
+                            str(seg), sfile, "1"])
+        os.remove(soa)
+        rec = dict(name=name, workload=workload, n=n, dim=dim, bits=bits, mode=mode, e=e, seg_in=seg, eb=eb)
+        if rc != 0:
+            rec["compress_error"] = (out + err).strip()[-400:]
+            recs.append(rec)
+            print(name, "compress failed", rc, err[-300:], flush=True)
+            continue
+        info = json.loads(out.strip().splitlines()[-1])
+        stream = np.fromfile(sfile, np.uint8)
+        rec.update(seg=info["seg"], adjusted=info["adjusted"], bytes=int(stream.size),
+                   stream_sha256=sha_array(stream), compress_ms=info["ms"])
+        del stream
+        dfile = os.path.join(tmp, "out.dec")
+        rc, out, err = run([HARNESS, "decompress", sfile, dfile, "1"])
+        if rc == 0:
+            dec = np.fromfile(dfile, np.uint8)
+            # the harness writes three axes; a 2D stream's third is zeros
+            rec["decoded_sha256"] = sha_array(dec[: dim * n * bits // 8])
+            rec["decompress_ms"] = json.loads(out.strip().splitlines()[-1])["ms"]
+            del dec
+            os.remove(dfile)
+        elif rc == 3:
+            rec["decompress_refused"] = out.strip()
+        else:
+            rec["decompress_error"] = (out + err).strip()[-400:]
+        os.remove(sfile)
+        recs.append(rec)
+        print(json.dumps(rec), flush=True)
+    with open(os.path.join(args.out, "full_size.json"), "w") as f:
+        json.dump(dict(fixtures=recs), f, indent=1)
+    shutil.rmtree(tmp, ignore_errors=True)
+
+
 def make_input(kind, n, dim, bits, lo, hi, seed, special):
     dtype = np.float32 if bits == 32 else np.float64
     x, y, z = po.generate(kind, n, dim, lo, hi, seed, dtype)
@@ -101,8 +192,12 @@ def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--out", required=True)
     ap.add_argument("--reps", type=int, default=1)
+    ap.add_argument("--full", action="store_true", help="record the full-size workloads (full_size.json)")
     args = ap.parse_args()
     os.makedirs(args.out, exist_ok=True)
+    if args.full:
+        main_full(args)
+        return
     tmp = tempfile.mkdtemp(prefix="gpz_golden_")
     fixtures = []
     for (name, kind, n, dim, bits, lo, hi, seed, mode, e, seg, special) in CASES:

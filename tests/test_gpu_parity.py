@@ -89,14 +89,27 @@ def run_arrays(x, y, z, dim, bits, mode, e, seg_in, safe31=False):
 def test_golden_case_bit_exact(f):
     s = run_case(f["kind"], f["n"], f["dim"], f["bits"], f["lo"], f["hi"], f["seed"], f["mode"], f["e"],
                  f["seg_in"], f["special"])
-    # and against the reference's own bytes, padding masked
+    # and against the reference's own bytes
     assert len(s) == f["bytes"]
-    if hashlib.sha256(s).hexdigest() != f["stream_sha256"] and "stream_file" in f:
+    if hashlib.sha256(s).hexdigest() == f["stream_sha256"]:
+        return
+    if "stream_file" in f:
+        # the reference leaves section padding unwritten (stale scratch): mask it
         ref = np.frombuffer(open(os.path.join(GOLD, f["stream_file"]), "rb").read(), np.uint8)
         ours = np.frombuffer(s, np.uint8)
         mask = po.padding_mask(ref)
         diff = np.nonzero(ours != ref)[0]
-        assert np.all(mask[diff] == 1)
+        assert np.all(mask[diff] == 1), f"non-padding bytes differ at {diff[mask[diff] == 0][:8]}"
+        assert np.all(ours[mask == 1] == 0)
+    else:
+        # stored as a hash only: below ~0.7M points the reference's padding
+        # holds its sampling temporaries, so the hashes may differ there; its
+        # own reconstruction then pins every other byte
+        assert "decoded_sha256" in f, "stream differs from the reference's and no reconstruction pins it"
+        dx, dy, dz = gz.decompress(_t(np.frombuffer(s, np.uint8)))
+        axes = (dx, dy, dz if dz is not None else torch.zeros_like(dx))
+        dec = b"".join(t.cpu().numpy().tobytes() for t in axes)
+        assert hashlib.sha256(dec).hexdigest() == f["decoded_sha256"]
 
 
 @pytest.mark.parametrize("f", [f for f in FIX if "stream_file" in f], ids=[f["name"] for f in FIX if "stream_file" in f])
