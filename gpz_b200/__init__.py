@@ -26,6 +26,7 @@ LIB_PATH = os.path.join(HERE, "libgpz_b200.so")
 GPZ_OK, GPZ_EINVAL, GPZ_ESEG, GPZ_ESTREAM, GPZ_ENOSPACE, GPZ_ECUDA, GPZ_ETIMEOUT, GPZ_ENOTSUP, GPZ_ELIMIT = range(9)
 GPZ_FLAG_SAFE31 = 1
 GPZ_FLAG_SEG_FIXED = 2
+GPZ_FLAG_STRICT_BOUND = 8
 GPZ_FLAG_REL_ON_DEVICE = 4
 GPZ_OP_COMPRESS, GPZ_OP_DECOMPRESS = 1, 2
 GPZ_SERVER_OVERLAP = 1
@@ -133,6 +134,7 @@ SIGNATURES = {
                                       ctypes.c_double, _U32, ctypes.POINTER(_U32), ctypes.POINTER(_U32)]),
     "gpz_rel_abs_from_minmax": (ctypes.c_int, [_U32, ctypes.POINTER(ctypes.c_double), ctypes.c_double,
                                                ctypes.POINTER(ctypes.c_double)]),
+    "gpz_strict_bound": (ctypes.c_int, [_U32, ctypes.c_double, ctypes.c_double, ctypes.POINTER(ctypes.c_double)]),
     "gpz_batch_create": (ctypes.c_int, [ctypes.POINTER(BatchItem), _U32, ctypes.POINTER(_VP), ctypes.POINTER(_U32)]),
     "gpz_batch_launch": (ctypes.c_int, [_VP, _VP]),
     "gpz_batch_results": (ctypes.c_int, [_VP, ctypes.POINTER(Result), ctypes.POINTER(ctypes.c_double), _VP]),
@@ -215,9 +217,18 @@ def compress_scratch_bytes(n: int) -> int:
 
 
 def make_params(n: int, dim: int, float_bits: int, eb: float, seg_size: int = 0, rel_mode: bool = False,
-                rel_eb: float = 0.0, safe31: bool = False) -> Params:
+                rel_eb: float = 0.0, safe31: bool = False, strict: bool = False) -> Params:
+    flags = (GPZ_FLAG_SAFE31 if safe31 else 0) | (GPZ_FLAG_STRICT_BOUND if strict else 0)
     return Params(float_bits=float_bits, dim=dim, n=n, eb=eb, rel_eb=rel_eb, rel_mode=1 if rel_mode else 0,
-                  seg_size=seg_size, flags=GPZ_FLAG_SAFE31 if safe31 else 0, reserved=0)
+                  seg_size=seg_size, flags=flags, reserved=0)
+
+
+def strict_bound(float_bits: int, eb: float, max_abs: float) -> float:
+    """The bound GPZ_FLAG_STRICT_BOUND encodes with for a snapshot whose largest
+    coordinate magnitude is max_abs (gpz_strict_bound)."""
+    out = ctypes.c_double()
+    _check(lib().gpz_strict_bound(float_bits, eb, max_abs, ctypes.byref(out)), "gpz_strict_bound")
+    return out.value
 
 
 def compress_into(params: Params, x, y, z, out, scratch, stream=None, sync: bool = True):
@@ -251,13 +262,13 @@ def result_post(scratch, host_result, stream=None):
 
 
 def compress(x, y, z=None, eb: float = 0.0, seg_size: int = 0, rel_mode: bool = False, rel_eb: float = 0.0,
-             safe31: bool = False, stream=None):
+             safe31: bool = False, stream=None, strict: bool = False):
     """Compresses SoA CUDA tensors; returns (stream bytes as a uint8 CUDA tensor, Result)."""
     torch = _torch()
     dim = 3 if z is not None else 2
     bits = _dtype_bits(x)
     n = x.numel()
-    p = make_params(n, dim, bits, eb, seg_size, rel_mode, rel_eb, safe31)
+    p = make_params(n, dim, bits, eb, seg_size, rel_mode, rel_eb, safe31, strict)
     out = torch.empty(stream_bound(n, dim, bits), dtype=torch.uint8, device=x.device)
     scratch = torch.empty(compress_scratch_bytes(n), dtype=torch.uint8, device=x.device)
     r = compress_into(p, x, y, z if dim == 3 else x, out, scratch, stream)

@@ -51,53 +51,58 @@ __global__ void __launch_bounds__(256) batch_sample_kernel(const BItem<T> *items
                       (it.flags & kBatchSafe31) ? 1 : 0, it.a.ctl, blockIdx.x, gridDim.x);
 }
 
-struct BatchGroup {
-  uint32_t sz[kEncWarps];     // payload bytes of each warp's chunk
-  unsigned long long goff;    // stream offset of the group (~0: look-back gave up)
-  unsigned long long next;    // next global group
-  unsigned long long nmap;    // its map entry
-};
-
 // The compress loop of compress_kernel over a work list of many snapshots:
-// map[g] = snapshot << 40 | group of global group g.  The arguments of the
-// current and the next group's snapshot live in shared memory (double
-// buffered: the next group's points are loaded during the current group's
-// look-back and copy-out).  A snapshot whose segment size could not be
-// chosen (sampling error, status set) is skipped as a whole.
+// map[g] = snapshot << 40 | group of global group g.  Each group slot also
+// holds its map entry and its snapshot's arguments (the next group's points
+// are loaded before the current group's offset is awaited).  A snapshot whose
+// segment size could not be chosen (sampling error, status set) is skipped as
+// a whole; a group whose look-back gave up is skipped and the loop goes on
+// with the other snapshots.
 template <typename T, int DIM>
 __global__ void __launch_bounds__(32 * kEncWarps, GPZ_ENC_MIN_CTAS)
     compress_batch_kernel(const BItem<T> *__restrict__ items, const unsigned long long *__restrict__ map,
                           unsigned long long total, unsigned long long *claim) {
   using Tr = TT<T>;
   constexpr bool is64 = sizeof(T) == 8;
-  constexpr uint32_t FULL = 0xFFFFFFFFu;
   constexpr unsigned long long kLocal = (1ull << kBatchLocalBits) - 1;
   extern __shared__ __align__(16) uint32_t enc_smem[];
-  __shared__ BatchGroup eg;
-  __shared__ CArgs<T> args[2];
+  __shared__ EncSlot slots[3];
+  __shared__ unsigned long long smap[3];
+  __shared__ CArgs<T> args[3];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   uint32_t *const sw = enc_smem + warp * kEncWords;
-  auto claim_next = [&](int slot) {  // thread 0
+  auto claim_into = [&](int j, uint32_t seq) {  // lane 0 of one warp
     const unsigned long long g = atomicAdd(claim, 1ull);
-    eg.next = g;
     // past the end: the first snapshot's first group stands in, so the
     // prefetch below needs no condition (its loads are never used)
     const unsigned long long m = g < total ? map[g] : 0ull;
-    eg.nmap = m;
-    args[slot] = items[m >> kBatchLocalBits].a;
+    slots[j].gbase = g;
+    slots[j].reported = 0;
+    slots[j].owner = 0;
+    slots[j].ready = 0;
+    smap[j] = m;
+    args[j] = items[m >> kBatchLocalBits].a;
+    __threadfence_block();
+    *reinterpret_cast<volatile uint32_t *>(&slots[j].seq) = seq;
   };
-  if (threadIdx.x == 0) claim_next(0);
+  Control *const ctl0 = items[0].a.ctl;  // where a batch-level wait that runs out is reported
+  if (threadIdx.x == 0) {
+    slots[1].seq = slots[2].seq = ~0u;
+    claim_into(0, 0u);
+  }
   __syncthreads();
   ChunkPoints<T, DIM> pts;
-  pts.load(args[0], (eg.nmap & kLocal) * kEncWarps + warp, lane);
-  int slot = 0;
-  for (;;) {
-    const unsigned long long g = eg.next;
+  pts.load(args[0], (smap[0] & kLocal) * kEncWarps + warp, lane);
+  int k = 0;
+  for (uint32_t it = 0;; ++it) {
+    EncSlot &s = slots[k];
+    const int k1 = k == 2 ? 0 : k + 1;
+    // a snapshot that aborts does not stop the others: no abort check here
+    if (!wait_claimed(s, it, ctl0, false)) break;
+    const unsigned long long g = *reinterpret_cast<volatile unsigned long long *>(&s.gbase);
     if (g >= total) break;
-    const unsigned long long m = eg.nmap;
-    __syncthreads();  // B0: everyone has the group before it is replaced
-    if (threadIdx.x == 0) claim_next(slot ^ 1);
-    const CArgs<T> &a = args[slot];
+    const unsigned long long m = *reinterpret_cast<volatile unsigned long long *>(&smap[k]);
+    const CArgs<T> &a = args[k];
     Control *ctl = a.ctl;
     const unsigned long long G = a.G;
     const unsigned long long gid = m & kLocal, gbase = gid * kEncWarps;
@@ -108,51 +113,17 @@ __global__ void __launch_bounds__(32 * kEncWarps, GPZ_ENC_MIN_CTAS)
     const T inv = is64 ? (T)__ddiv_rn(1.0, __dmul_rn(2.0, (double)eb)) : (T)__fdiv_rn(1.0f, __fmul_rn(2.0f, (float)eb));
     const unsigned long long pay_base = Tr::hdr + 8ull * G + (unsigned long long)Tr::meta * G;
     const unsigned long long c = gbase + warp;
+    auto on_size = [&](uint32_t bytes) { report_size(s, bytes, warp, lane, [&]() { claim_into(k1, it + 1); }); };
     uint32_t payload = 0, meta_word = 0;
-    if (live && c < G) payload = encode_chunk<T, DIM>(a, c, sw, seg, sh, msk, inv, pts, meta_word, lane);
-    if (lane == 0) eg.sz[warp] = payload;
-    __syncthreads();  // B1: the group's sizes are known (and the next group's snapshot)
-    pts.load(args[slot ^ 1], (eg.nmap & kLocal) * kEncWarps + warp, lane);  // in flight during the look-back and copy-out
-    if (live && warp == 0) {
-      const uint32_t s = lane < kEncWarps ? eg.sz[lane] : 0u;
-      const uint32_t tot = __reduce_add_sync(FULL, s);
-      if (lane == 0) publish_aggregate(a.look, gid, tot);
-      unsigned long long excl = 0;
-      const bool ok = resolve_prefix(a.look, gid, tot, ctl, excl);
-      if (lane == 0) eg.goff = ok ? excl : ~0ull;
-    }
-    __syncthreads();  // B2: the group's stream offset is known
-    const unsigned long long goff = eg.goff;
-    if (live && c < G && goff != ~0ull) {
-      unsigned long long off = goff;
-      for (int w = 0; w < warp; ++w) off += eg.sz[w];
-      if (lane == 0) reinterpret_cast<unsigned long long *>(a.out + Tr::hdr)[c] = off;
-      uint8_t *meta = a.out + Tr::hdr + 8ull * G + (unsigned long long)Tr::meta * c;
-      if (lane < (int)(Tr::meta / 4)) reinterpret_cast<uint32_t *>(meta)[lane] = meta_word;
-      if (c == 0) {
-        uint32_t *h = reinterpret_cast<uint32_t *>(a.out);
-        if (lane == 0) h[0] = a.dim;
-        if (lane == 1) h[1] = (uint32_t)a.n;
-        if (lane == 2) h[2] = (uint32_t)(a.n >> 32);
-        if (lane == 3) h[3] = Tr::bits;
-        if (!is64) {
-          if (lane == 4) h[4] = __float_as_uint((float)a.eb);
-          if (lane == 5) h[5] = seg;
-        } else {
-          if (lane == 4) h[4] = (uint32_t)__double_as_longlong((double)a.eb);
-          if (lane == 5) h[5] = (uint32_t)((unsigned long long)__double_as_longlong((double)a.eb) >> 32);
-          if (lane == 6) h[6] = seg;
-          if (lane == 7) h[7] = 32u;
-        }
-      }
-      if (pay_base + off + payload > a.out_cap) {
-        if (lane == 0) set_status(ctl, kENOSPACE);
-      } else {
-        copy_payload(reinterpret_cast<uint32_t *>(a.out + pay_base + off), sw, payload, lane);
-      }
-      if (c == G - 1 && lane == 0) ctl->stream_bytes = pay_base + off + payload;
-    }
-    slot ^= 1;
+    if (live && c < G) payload = encode_chunk<T, DIM>(a, c, sw, seg, sh, msk, eb, inv, pts, meta_word, lane, on_size);
+    else on_size(0u);
+    if (!wait_claimed(slots[k1], it + 1, ctl0, false)) break;
+    pts.load(args[k1], (*reinterpret_cast<volatile unsigned long long *>(&smap[k1]) & kLocal) * kEncWarps + warp,
+             lane);
+    if (place_offset(s, live, gid, a.look, ctl, lane) && c < G)
+      place_chunk<T>(a, c, G, pay_base, chunk_offset(s, warp), payload, meta_word, seg, eb, sw, lane);
+    __syncwarp();  // the staged payload is read before the region is reused
+    k = k1;
   }
 }
 

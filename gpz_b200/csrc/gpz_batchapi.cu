@@ -48,6 +48,7 @@ void fill_item(BItem<T> &bi, const gpz_batch_item &it, uint8_t *dev, uint64_t ct
   bi.a.n = it.n;
   bi.a.G = chunks_of(it.n);
   bi.a.eb = (T)it.eb;
+  bi.a.eb_dev = nullptr;
   bi.a.dim = it.dim;
   auto al = [](const void *p) { return ((uintptr_t)p & 15u) == 0; };
   bi.a.vec_ok = al(it.d_x) && al(it.d_y) && (it.dim == 2 || al(it.d_z));

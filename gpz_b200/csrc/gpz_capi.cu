@@ -66,12 +66,19 @@ int compress_t(const gpz_params *p, const void *d_x, const void *d_y, const void
   const T eb = (T)p->eb;
   const T rel = (T)p->rel_eb;
   const T *x = static_cast<const T *>(d_x), *y = static_cast<const T *>(d_y), *z = static_cast<const T *>(d_z);
+  // strict-bound mode: the bound actually encoded is shrunk on the device by
+  // the reconstruction's worst rounding over the snapshot's magnitude range
+  const bool strict = (p->flags & GPZ_FLAG_STRICT_BOUND) != 0;
+  const double *eb_dev = strict ? &ctl->strict_eb : nullptr;
+  if (strict)
+    strict_bound_kernel<T><<<num_sms() * 4, 256, 0, st>>>(x, y, p->dim == 3 ? z : y, p->n, p->dim, eb, ctl);
   if (p->flags & GPZ_FLAG_SEG_FIXED) {
     if (p->seg_size == 0) return GPZ_EINVAL;
     set_seg_kernel<<<1, 1, 0, st>>>(ctl, p->seg_size);
   } else {
+    const int safe31 = (p->flags & (GPZ_FLAG_SAFE31 | GPZ_FLAG_STRICT_BOUND)) ? 1 : 0;
     seg_sample_kernel<T><<<128, 256, 0, st>>>(x, y, p->dim == 3 ? z : y, p->n, p->dim, p->seg_size, p->rel_mode, rel,
-                                              eb, (p->flags & GPZ_FLAG_SAFE31) ? 1 : 0, ctl);
+                                              eb, safe31, ctl, eb_dev);
   }
   CArgs<T> a;
   a.x = x; a.y = y; a.z = p->dim == 3 ? z : y;
@@ -82,6 +89,7 @@ int compress_t(const gpz_params *p, const void *d_x, const void *d_y, const void
   a.n = p->n;
   a.G = G;
   a.eb = eb;
+  a.eb_dev = eb_dev;
   a.dim = p->dim;
   a.vec_ok = aligned16(d_x) && aligned16(d_y) && (p->dim == 2 || aligned16(d_z));
   // persistent grid: one CTA per kEncWarps chunks in flight
@@ -391,6 +399,15 @@ int gpz_decide_seg(uint32_t float_bits, uint32_t dim, const uint64_t *acc6, uint
   if (sd.status != kOK) return sd.status;
   *seg = sd.seg;
   *adjusted = sd.adjusted;
+  return GPZ_OK;
+}
+
+int gpz_strict_bound(uint32_t float_bits, double eb, double max_abs, double *eb_strict) {
+  if ((float_bits != 32 && float_bits != 64) || !eb_strict || !(eb > 0.0) || !(max_abs >= 0.0)) return GPZ_EINVAL;
+  const double e = float_bits == 32 ? (double)strict_bound<float>((float)eb, (float)max_abs)
+                                    : strict_bound<double>(eb, max_abs);
+  if (!(e > 0.0)) return GPZ_EINVAL;
+  *eb_strict = e;
   return GPZ_OK;
 }
 

@@ -63,6 +63,9 @@ void print_usage(const char *prog) {
             << "        -e <float>       [Required if -t used] Error bound\n"
             << "        -f <int>         [Required if -t used] Float bits (32 or 64)\n"
             << "        -p <dim>         [Optional] Number of dimensions (default: 3)\n"
+            << "\n"
+            << "  Extension (not in the reference):\n"
+            << "        -B               [Optional, compress] Hold the error bound for every point (strict-bound mode)\n"
             << std::endl;
 }
 
@@ -241,9 +244,56 @@ void verify(const T *d_dec, const char *original, uint64_t n, uint32_t dim, doub
   printf("PSNR: %f\n", combine_psnr(psnrs));
 }
 
+// -B (an extension): strict-bound mode through the C ABI
+// (GPZ_FLAG_STRICT_BOUND): the stream holds the stated bound for every
+// finite point; its header carries the shrunk bound actually encoded.
+template <typename T>
+int run_compress_strict(const Pinned &aos, const Device &d_aos, const Device &d_xyz, const char *out, uint64_t n,
+                        uint32_t dim, const std::string &mode, double bound, double input_bound, uint32_t seg) {
+  gpz_params p;
+  memset(&p, 0, sizeof(p));
+  p.float_bits = sizeof(T) * 8;
+  p.dim = dim;
+  p.n = n;
+  p.eb = bound;
+  p.rel_eb = input_bound;
+  p.rel_mode = mode == "rel" ? 1 : 0;
+  p.seg_size = seg;
+  p.flags = GPZ_FLAG_STRICT_BOUND;
+  const uint64_t cap = gpz_stream_bound(n, dim, p.float_bits), scr_bytes = gpz_compress_scratch_bytes(n);
+  Device d_out(cap), scr(scr_bytes);
+  const T *x = static_cast<const T *>(d_xyz.p);
+  gpz_result r;
+  for (int i = 0; i < 5; ++i)  // warm up, as the reference CLI does (src/main.cpp:300-321)
+    gpz_ok(gpz_compress(&p, x, x + n, x + 2 * n, d_out.p, cap, scr.p, scr_bytes, &r, nullptr), "gpz_compress");
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  cudaEventRecord(e0);
+  gpz_ok(gpz_compress_async(&p, x, x + n, x + 2 * n, d_out.p, cap, scr.p, scr_bytes, nullptr), "gpz_compress_async");
+  cudaEventRecord(e1);
+  cudaEventSynchronize(e1);
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, e0, e1);
+  gpz_ok(gpz_result_get(scr.p, &r, nullptr), "gpz_result_get");
+  Pinned h_stream(r.stream_bytes);
+  cuda_ok(cudaMemcpy(h_stream.p, d_out.p, r.stream_bytes, cudaMemcpyDeviceToHost), "download");
+  double eb_enc = 0.0;
+  uint32_t d2, b2, s2;
+  uint64_t n2;
+  gpz_ok(gpz_parse_header(h_stream.p, r.stream_bytes, &d2, &n2, &b2, &eb_enc, &s2), "gpz_parse_header");
+  printf("Strict bound: encoded with eb %.10g (stated %.10g)\n", eb_enc, (double)(T)bound);
+  write_file(out, h_stream.p, r.stream_bytes);
+  CudaConfig cfg(r.seg_size, r.adjusted != 0, dim, n, mode, (float)bound, (float)input_bound, p.float_bits);
+  print_compression_result(r.stream_bytes, n * dim * sizeof(T), 1024.0 * 1024.0 * 1024.0, ms, cfg);
+  (void)aos;
+  (void)d_aos;
+  return 0;
+}
+
 template <typename T>
 int run_compress(const char *in, const char *out, uint64_t n, uint32_t dim, const std::string &mode, double bound,
-                 uint32_t seg, const std::string &nvcomp_type) {
+                 uint32_t seg, const std::string &nvcomp_type, bool strict) {
   const uint64_t aos_bytes = n * dim * sizeof(T), xyz_bytes = 3 * n * sizeof(T);
   check_points_file<T>(in, n, dim);
   Pinned aos(aos_bytes);
@@ -267,6 +317,7 @@ int run_compress(const char *in, const char *out, uint64_t n, uint32_t dim, cons
     printf("Max Range is: %.10g\n", (double)range);
     printf("Abs Error bound: %.10g\n", (double)(T)bound);
   }
+  if (strict) return run_compress_strict<T>(aos, d_aos, d_xyz, out, n, dim, mode, bound, input_bound, seg);
   ICudaCompressor *codec;
   if (sizeof(T) == 4)
     codec = new CudaWarpCompress(CudaConfig(seg, false, dim, n, mode, (float)bound, (float)input_bound, 32u));
@@ -352,10 +403,10 @@ int main(int argc, char *argv[]) {
   uint32_t float_bits = 0, dim = 3, segment_size = 0;
   double error_bound = 0.0;
   std::string err_mode, nvcomp_type = "none";
-  bool compress_mode = false, decompress_mode = false, verification_mode = false;
+  bool compress_mode = false, decompress_mode = false, verification_mode = false, strict = false;
   int opt;
   try {
-    while ((opt = getopt(argc, argv, "xdi:o:p:n:e:s:m:f:t:r:v:h")) != -1) {
+    while ((opt = getopt(argc, argv, "xdi:o:p:n:e:s:m:f:t:r:v:hB")) != -1) {
       switch (opt) {
         case 'x': compress_mode = true; break;
         case 'd': decompress_mode = true; break;
@@ -370,6 +421,7 @@ int main(int argc, char *argv[]) {
         case 't': nvcomp_type = optarg; break;
         case 'r': recon_filename = optarg; break;
         case 'v': verification_mode = true; original_filename = optarg; break;
+        case 'B': strict = true; break;
         case 'h':
         default: print_usage(argv[0]); return 1;
       }
@@ -428,9 +480,9 @@ int main(int argc, char *argv[]) {
     if (compress_mode) {
       return float_bits == 32
                  ? run_compress<float>(filename, output_filename, num_points, dim, err_mode, error_bound, segment_size,
-                                       nvcomp_type)
+                                       nvcomp_type, strict)
                  : run_compress<double>(filename, output_filename, num_points, dim, err_mode, error_bound,
-                                        segment_size, nvcomp_type);
+                                        segment_size, nvcomp_type, strict);
     }
     // decompress: -o is the compressed input, -r the reconstructed output (src/main.cpp:378-390)
     uint64_t data_size = 0;

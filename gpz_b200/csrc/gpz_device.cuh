@@ -37,6 +37,7 @@ struct Control {
   double out_eb;                    // 88  rel->abs result
   double out_mm[6];                 // 96  rel->abs min/max
   uint64_t G;                       // 144 chunks (decompress: from the header)
+  double strict_eb;                 // 152 bound actually encoded in strict-bound mode
 };
 static_assert(sizeof(Control) <= kCtlBytes, "control block too large");
 

@@ -19,10 +19,14 @@
 //      arrival slot, multi-point buckets put in order afterwards);
 //   3. finds the runs of equal ids (unique ids, deltas, counts) and compacts
 //      them through shared memory so lane l holds runs 32l..32l+31;
-//   4. transposes deltas, counts and relative positions into bit planes in
-//      registers and assembles the payload in its shared region.
-// The 8 warps of a CTA take 8 consecutive chunks together; one decoupled
-// look-back per group places the group's payloads in the stream.
+//   4. reports its payload size, then transposes deltas, counts and relative
+//      positions into bit planes in registers and assembles the payload in
+//      its shared region.
+// The 8 warps of a CTA take 8 consecutive chunks (a group) together, with no
+// CTA-wide barrier in the loop: the first warp to report a size claims the
+// next group, the first warp to finish its planes resolves the group's
+// stream offset (one decoupled look-back per group) while slower warps still
+// build theirs, and each warp copies its payload out once the offset is known.
 #pragma once
 
 #include <cfloat>
@@ -43,10 +47,18 @@ constexpr int kEncSmall = 16;             // buckets of this many points or more
 constexpr int kEncWords = 3 * kChunk;     // per-warp shared words (12 KB)
 static_assert(kStageBytes <= kEncWords * 4, "payload staging must fit the warp region");
 
-struct EncGroup {
+// Per-CTA state of one group of kEncWarps consecutive chunks.  Three slots
+// rotate: the group being encoded, the next one (claimed by the first warp to
+// report a size in the current one) and the previous one (still being copied
+// out by slower warps).
+struct EncSlot {
+  unsigned long long gbase;  // first chunk of the group (>= G: no more work)
+  uint32_t seq;              // loop iteration whose group the slot holds (set last by the claimer)
+  unsigned long long goff;   // stream offset of the group's payloads (~0: the look-back gave up)
   uint32_t sz[kEncWarps];    // payload bytes of each warp's chunk
-  unsigned long long goff;   // stream offset of the group (~0: look-back gave up)
-  unsigned long long next;   // first chunk of the next group
+  uint32_t reported;         // warps whose size is in sz
+  uint32_t owner;            // set by the warp that resolves the group's offset
+  uint32_t ready;            // goff is final
 };
 
 constexpr size_t enc_smem_bytes() { return (size_t)kEncWarps * kEncWords * 4; }
@@ -96,24 +108,10 @@ __host__ __device__ __forceinline__ void oem_sort32(uint32_t (&a)[32]) {
           }
 }
 
-// Merges two ascending halves a[0..15], a[16..31] (bitonic merge: the first
-// stage compares mirrored positions, then half-cleaners).
-__host__ __device__ __forceinline__ void merge_halves32(uint32_t (&a)[32]) {
-#pragma unroll
-  for (int i = 0; i < 16; ++i) {
-    const uint32_t x = a[i], y = a[31 - i];
-    a[i] = x < y ? x : y;
-    a[31 - i] = x < y ? y : x;
-  }
-#pragma unroll
-  for (int s = 8; s >= 1; s >>= 1)
-#pragma unroll
-    for (int i = 0; i < 32; ++i)
-      if ((i & s) == 0) {
-        const uint32_t x = a[i], y = a[i + s];
-        a[i] = x < y ? x : y;
-        a[i + s] = x < y ? y : x;
-      }
+__device__ __forceinline__ void cas_up(uint32_t &x, uint32_t &y) {
+  const uint32_t lo = min(x, y);
+  y = max(x, y);
+  x = lo;
 }
 
 // Row <-> column transposes of the warp's 32x32 value matrix through a
@@ -143,11 +141,6 @@ __device__ __forceinline__ void columns_to_rows(uint32_t (&v)[32], uint32_t *tsm
   }
 }
 
-__device__ __forceinline__ void cas_up(uint32_t &x, uint32_t &y) {
-  const uint32_t lo = min(x, y);
-  y = max(x, y);
-  x = lo;
-}
 
 // Ascending sort of the warp's 1024 values held in the swizzled rows `rows`
 // (lane l: elements 32l..32l+31), in place; tsm is a second 1024-word scratch.  Bitonic sort in the variant whose comparators
@@ -499,13 +492,12 @@ struct ChunkPoints {
 // 8 KB still hold the previous chunk's staged payload.
 template <typename T, int DIM>
 __device__ __forceinline__ void encode_quantize(const CArgs<T> &a, unsigned long long c, uint32_t *sw,
-                                                uint32_t seg, uint32_t sh, uint32_t msk, T inv,
+                                                uint32_t seg, uint32_t sh, uint32_t msk, T eb, T inv,
                                                 ChunkPoints<T, DIM> &pts, ChunkQ &q, int lane) {
   using Tr = TT<T>;
   using UO = typename Tr::U;
   constexpr bool is64 = sizeof(T) == 8;
   constexpr uint32_t FULL = 0xFFFFFFFFu;
-  const T eb = a.eb;
   const unsigned long long n = a.n;
   const unsigned long long base = c * kChunk;
   const uint32_t nvalid = (uint32_t)min((unsigned long long)kChunk, n - base);
@@ -631,9 +623,9 @@ __device__ __forceinline__ void encode_quantize(const CArgs<T> &a, unsigned long
 // ids in q and its relative positions in the warp's third 4 KB); stages the
 // payload in the warp's region, returns its bytes and leaves the meta record
 // in meta_word (word k of the record in lane k).
-template <typename T, int DIM>
+template <typename T, int DIM, class OnSize>
 __device__ __forceinline__ uint32_t encode_pack(const CArgs<T> &a, unsigned long long c, uint32_t *sw, ChunkQ &q,
-                                                uint32_t &meta_word, int lane) {
+                                                uint32_t &meta_word, int lane, OnSize &&on_size) {
   using Tr = TT<T>;
   constexpr bool is64 = sizeof(T) == 8;
   constexpr uint32_t FULL = 0xFFFFFFFFu;
@@ -653,24 +645,16 @@ __device__ __forceinline__ uint32_t encode_pack(const CArgs<T> &a, unsigned long
   uint32_t rp[16];  // rank r of positions j and j+16 (16-bit pairs)
   if (cbits_all <= 32u) {
     // 32-bit composites: one data-independent warp sort.  Slots past the
-    // chunk's end take the largest composite, (kmax - kmin) << 10 | 1023: no
-    // point of a short chunk has r = 1023, so they sort last, and they carry
-    // the last id kmax, so they start no run.
+    // chunk's end (point 32j + lane >= nvalid) take the largest
+    // composite, (kmax - kmin) << 10 | 1023: no point of a short chunk has
+    // r = 1023, so they sort last, and they carry the last id kmax, so they
+    // start no run.
 #pragma unroll
-    for (int m = 0; m < 8; ++m) {
-      uint32_t cv[4];
+    for (int j = 0; j < 32; ++j)
+      key[j] = (full || 32u * j + lane < nvalid) ? (((key[j] - kmin) << 10) | (32u * lane + j)) : (uint32_t)cmax;
 #pragma unroll
-      for (int e = 0; e < 4; ++e) {
-        const int j = 4 * m + e;
-        cv[e] = ((key[j] - kmin) << 10) | (32u * lane + j);
-      }
-      *reinterpret_cast<uint4 *>(S + qoff(lane, m)) = make_uint4(cv[0], cv[1], cv[2], cv[3]);
-    }
-    if (!full) {
-#pragma unroll 1
-      for (int j = 0; j < 32; ++j)
-        if (32u * j + lane >= nvalid) S[qoff(lane, j >> 2) + (j & 3)] = (uint32_t)cmax;
-    }
+    for (int m = 0; m < 8; ++m)
+      *reinterpret_cast<uint4 *>(S + qoff(lane, m)) = make_uint4(key[4 * m], key[4 * m + 1], key[4 * m + 2], key[4 * m + 3]);
     warp_sort1024_rows(S, hist, lane);
 #pragma unroll
     for (int m = 0; m < 8; ++m) {
@@ -789,6 +773,7 @@ __device__ __forceinline__ uint32_t encode_pack(const CArgs<T> &a, unsigned long
   // ---- 4. bit planes -> staged payload (:313-411) ----
   const uint32_t db = section_bytes(U, dbits, Tr::pad), cb = section_bytes(U, cbits, Tr::pad);
   const uint32_t rb = rel_section_bytes(rbits, Tr::pad);
+  on_size(db + cb + rb);  // the payload size is known before its planes are built
   const uint32_t bpp = (U + 7u) >> 3;
   uint32_t *const stage = sw;
   put_planes(stage, 0u, dbits, bpp, dl, lane);
@@ -838,13 +823,16 @@ __device__ __forceinline__ uint32_t encode_pack(const CArgs<T> &a, unsigned long
 
 // Encodes chunk c into the warp's region `sw`; returns the payload bytes and
 // leaves the meta record in meta_word (word k of the record in lane k).
-template <typename T, int DIM>
+// on_size(bytes) runs (warp-wide) as soon as the payload size is known, before
+// the bit planes are built.
+template <typename T, int DIM, class OnSize>
 __device__ __forceinline__ uint32_t encode_chunk(const CArgs<T> &a, unsigned long long c, uint32_t *sw,
-                                                 uint32_t seg, uint32_t sh, uint32_t msk, T inv,
-                                                 ChunkPoints<T, DIM> &pts, uint32_t &meta_word, int lane) {
+                                                 uint32_t seg, uint32_t sh, uint32_t msk, T eb, T inv,
+                                                 ChunkPoints<T, DIM> &pts, uint32_t &meta_word, int lane,
+                                                 OnSize &&on_size) {
   ChunkQ q;
-  encode_quantize<T, DIM>(a, c, sw, seg, sh, msk, inv, pts, q, lane);
-  return encode_pack<T, DIM>(a, c, sw, q, meta_word, lane);
+  encode_quantize<T, DIM>(a, c, sw, seg, sh, msk, eb, inv, pts, q, lane);
+  return encode_pack<T, DIM>(a, c, sw, q, meta_word, lane, on_size);
 }
 
 // Copies a staged payload (whole words) to its place in the stream: four
@@ -865,80 +853,201 @@ __device__ __forceinline__ void copy_payload(uint32_t *dst, const uint32_t *sw, 
   }
 }
 
+// Group bookkeeping shared by the plain and batched compress kernels.
+//
+// report_size: this warp's payload size for the group in slot s, reported as
+// soon as it is known (before the bit planes are built).  The first warp of
+// the CTA to report claims the next group (claim_next(), lane 0): it fills
+// the slot of the group before the previous one, which no warp uses any more
+// (a warp enters a group only after every warp has reported in the group
+// before it), and sets the slot's seq last.  Warp-collective.
+template <class ClaimNext>
+__device__ __forceinline__ void report_size(EncSlot &s, uint32_t bytes, int warp, int lane, ClaimNext &&claim_next) {
+  if (lane == 0) {
+    s.sz[warp] = bytes;
+    __threadfence_block();
+    if (atomicAdd(&s.reported, 1u) == 0u) claim_next();
+  }
+  __syncwarp();
+}
+
+// Waits (bounded) until slot s holds the group of loop iteration `seq`; a
+// wait that runs out (or, with check_abort, another CTA's abort) is reported
+// in ctl.
+__device__ __forceinline__ bool wait_claimed(const EncSlot &s, uint32_t seq, Control *ctl, bool check_abort = true) {
+  uint32_t spins = 0;
+  while (ld_volatile(&s.seq) != seq) {
+    if (++spins > 4u * kSpinLimit || (check_abort && (spins & 63u) == 0u && ld_volatile(&ctl->abort))) {
+      if ((threadIdx.x & 31) == 0) {
+        atomicExch(&ctl->abort, 1u);
+        set_status(ctl, kETIMEOUT);
+      }
+      return false;
+    }
+    __nanosleep(64);
+  }
+  __threadfence_block();
+  return true;
+}
+
+// place_offset: the group's stream offset, once this warp's payload is staged.
+// The first warp to get here owns the group: it waits (bounded) for the other
+// warps' sizes, publishes the group's aggregate, resolves its offset by
+// decoupled look-back (bounded; skipped when !live) and releases it.  The
+// others wait (bounded) for it.  So the look-back runs on a warp that has
+// nothing else to do, while slower warps still build their planes.  Returns
+// false when the group is not placed (look-back gave up, another CTA aborted,
+// or a wait ran out).  Warp-collective.
+__device__ __forceinline__ bool place_offset(EncSlot &s, bool live, unsigned long long gid, unsigned long long *look,
+                                             Control *ctl, int lane) {
+  constexpr uint32_t FULL = 0xFFFFFFFFu;
+  uint32_t own = 0;
+  if (lane == 0) own = atomicCAS(&s.owner, 0u, 1u) == 0u;
+  own = __shfl_sync(FULL, own, 0);
+  auto give_up = [&]() {
+    if (lane == 0) {
+      atomicExch(&ctl->abort, 1u);
+      set_status(ctl, kETIMEOUT);
+    }
+  };
+  if (own) {
+    uint32_t spins = 0, backoff = 32;
+    bool ok = true;
+    while (ld_volatile(&s.reported) < (uint32_t)kEncWarps) {
+      if (++spins > 2u * kSpinLimit || ((spins & 63u) == 0u && ld_volatile(&ctl->abort))) {
+        give_up();
+        ok = false;
+        break;
+      }
+      __nanosleep(backoff);
+      backoff = min(backoff * 2, 256u);
+    }
+    __threadfence_block();
+    unsigned long long excl = 0;
+    if (ok && live) {
+      const uint32_t v = lane < kEncWarps ? ld_volatile(&s.sz[lane]) : 0u;
+      const uint32_t total = __reduce_add_sync(FULL, v);
+      if (lane == 0) publish_aggregate(look, gid, total);
+      ok = resolve_prefix(look, gid, total, ctl, excl);
+    }
+    if (lane == 0) {
+      s.goff = ok && live ? excl : ~0ull;
+      __threadfence_block();
+      *reinterpret_cast<volatile uint32_t *>(&s.ready) = 1u;
+    }
+    __syncwarp();
+    return ok && live;
+  }
+  uint32_t spins = 0, backoff = 32;
+  while (ld_volatile(&s.ready) == 0u) {
+    if (++spins > 4u * kSpinLimit || ((spins & 63u) == 0u && ld_volatile(&ctl->abort))) {
+      give_up();
+      return false;
+    }
+    __nanosleep(backoff);
+    backoff = min(backoff * 2, 256u);
+  }
+  __threadfence_block();
+  return *reinterpret_cast<const volatile unsigned long long *>(&s.goff) != ~0ull;
+}
+
+// Stream offset of warp w's chunk in a placed group.
+__device__ __forceinline__ unsigned long long chunk_offset(const EncSlot &s, int warp) {
+  unsigned long long off = *reinterpret_cast<const volatile unsigned long long *>(&s.goff);
+  for (int w = 0; w < warp; ++w) off += ld_volatile(&s.sz[w]);
+  return off;
+}
+
+// Writes a placed chunk: its offset-table entry (:1679), meta record, payload,
+// and for chunk 0 the header (:1674-1678; Double :1672-1680).
+template <typename T>
+__device__ __forceinline__ void place_chunk(const CArgs<T> &a, unsigned long long c, unsigned long long G,
+                                            unsigned long long pay_base, unsigned long long off, uint32_t payload,
+                                            uint32_t meta_word, uint32_t seg, T eb, const uint32_t *sw, int lane) {
+  using Tr = TT<T>;
+  constexpr bool is64 = sizeof(T) == 8;
+  if (lane == 0) reinterpret_cast<unsigned long long *>(a.out + Tr::hdr)[c] = off;
+  uint8_t *meta = a.out + Tr::hdr + 8ull * G + (unsigned long long)Tr::meta * c;
+  if (lane < (int)(Tr::meta / 4)) reinterpret_cast<uint32_t *>(meta)[lane] = meta_word;
+  if (c == 0) {
+    uint32_t *h = reinterpret_cast<uint32_t *>(a.out);
+    if (lane == 0) h[0] = a.dim;
+    if (lane == 1) h[1] = (uint32_t)a.n;
+    if (lane == 2) h[2] = (uint32_t)(a.n >> 32);
+    if (lane == 3) h[3] = Tr::bits;
+    if (!is64) {
+      if (lane == 4) h[4] = __float_as_uint((float)eb);
+      if (lane == 5) h[5] = seg;
+    } else {
+      if (lane == 4) h[4] = (uint32_t)__double_as_longlong((double)eb);
+      if (lane == 5) h[5] = (uint32_t)((unsigned long long)__double_as_longlong((double)eb) >> 32);
+      if (lane == 6) h[6] = seg;
+      if (lane == 7) h[7] = 32u;
+    }
+  }
+  if (pay_base + off + payload > a.out_cap) {
+    if (lane == 0) set_status(a.ctl, kENOSPACE);
+  } else {
+    copy_payload(reinterpret_cast<uint32_t *>(a.out + pay_base + off), sw, payload, lane);
+  }
+  if (c == G - 1 && lane == 0) a.ctl->stream_bytes = pay_base + off + payload;
+}
+
+// Persistent compress kernel: every CTA encodes groups of kEncWarps
+// consecutive chunks, one chunk per warp.  No CTA-wide barrier inside the
+// loop: a warp reports its payload size as soon as it is known, the last
+// reporter resolves the group's offset while the others build their bit
+// planes, and each warp then waits only for that offset before copying its
+// staged payload out.  Warps of a CTA are at most one group apart.
 template <typename T, int DIM>
 __global__ void __launch_bounds__(32 * kEncWarps, GPZ_ENC_MIN_CTAS) compress_kernel(const CArgs<T> a) {
   using Tr = TT<T>;
   constexpr bool is64 = sizeof(T) == 8;
-  constexpr uint32_t FULL = 0xFFFFFFFFu;
   extern __shared__ __align__(16) uint32_t enc_smem[];
-  __shared__ EncGroup eg;
+  __shared__ EncSlot slots[3];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   uint32_t *const sw = enc_smem + warp * kEncWords;
   Control *ctl = a.ctl;
   if (ld_volatile(reinterpret_cast<const uint32_t *>(&ctl->status)) != 0) return;
   const uint32_t seg = ctl->seg;
   const uint32_t sh = (uint32_t)__ffs((int)seg) - 1u, msk = seg - 1u;
-  const T eb = a.eb;
+  const T eb = a.eb_dev ? (T)*a.eb_dev : a.eb;
   const T inv = is64 ? (T)__ddiv_rn(1.0, __dmul_rn(2.0, (double)eb)) : (T)__fdiv_rn(1.0f, __fmul_rn(2.0f, (float)eb));
   const unsigned long long G = a.G;
   const unsigned long long pay_base = Tr::hdr + 8ull * G + (unsigned long long)Tr::meta * G;
-
-  if (threadIdx.x == 0) eg.next = atomicAdd(&ctl->chunk_ctr, (uint32_t)kEncWarps);
+  auto claim_into = [&](EncSlot &t, uint32_t seq) {  // lane 0 of one warp
+    t.gbase = ld_volatile(&ctl->abort) ? G : (unsigned long long)atomicAdd(&ctl->chunk_ctr, (uint32_t)kEncWarps);
+    t.reported = 0;
+    t.owner = 0;
+    t.ready = 0;
+    __threadfence_block();
+    *reinterpret_cast<volatile uint32_t *>(&t.seq) = seq;
+  };
+  if (threadIdx.x == 0) {
+    slots[1].seq = slots[2].seq = ~0u;
+    claim_into(slots[0], 0u);
+  }
   __syncthreads();
   ChunkPoints<T, DIM> pts;
-  pts.load(a, eg.next + warp, lane);
-  for (;;) {
-    const unsigned long long gbase = eg.next;
+  pts.load(a, slots[0].gbase + warp, lane);
+  int k = 0;
+  for (uint32_t it = 0;; ++it) {
+    EncSlot &s = slots[k];
+    const int k1 = k == 2 ? 0 : k + 1;
+    if (!wait_claimed(s, it, ctl)) break;
+    const unsigned long long gbase = *reinterpret_cast<volatile unsigned long long *>(&s.gbase);
     if (gbase >= G) break;
-    __syncthreads();  // B0: everyone has the group before it is replaced
-    if (threadIdx.x == 0) eg.next = ld_volatile(&ctl->abort) ? G : atomicAdd(&ctl->chunk_ctr, (uint32_t)kEncWarps);
-    const unsigned long long c = gbase + warp;
+    const unsigned long long c = gbase + warp, gid = gbase / kEncWarps;
+    auto on_size = [&](uint32_t bytes) { report_size(s, bytes, warp, lane, [&]() { claim_into(slots[k1], it + 1); }); };
     uint32_t payload = 0, meta_word = 0;
-    if (c < G) payload = encode_chunk<T, DIM>(a, c, sw, seg, sh, msk, inv, pts, meta_word, lane);
-    if (lane == 0) eg.sz[warp] = payload;
-    __syncthreads();  // B1: the group's sizes are known (and the next group's id)
-    pts.load(a, eg.next + warp, lane);  // in flight during the look-back and copy-out
-    if (warp == 0) {
-      const uint32_t s = lane < kEncWarps ? eg.sz[lane] : 0u;
-      const uint32_t total = __reduce_add_sync(FULL, s);
-      const unsigned long long gid = gbase / kEncWarps;
-      if (lane == 0) publish_aggregate(a.look, gid, total);
-      unsigned long long excl = 0;
-      const bool ok = resolve_prefix(a.look, gid, total, ctl, excl);
-      if (lane == 0) eg.goff = ok ? excl : ~0ull;
-    }
-    __syncthreads();  // B2: the group's stream offset is known
-    const unsigned long long goff = eg.goff;
-    if (c < G && goff != ~0ull) {
-      unsigned long long off = goff;
-      for (int w = 0; w < warp; ++w) off += eg.sz[w];
-      if (lane == 0) reinterpret_cast<unsigned long long *>(a.out + Tr::hdr)[c] = off;  // :1679
-      uint8_t *meta = a.out + Tr::hdr + 8ull * G + (unsigned long long)Tr::meta * c;
-      if (lane < (int)(Tr::meta / 4)) reinterpret_cast<uint32_t *>(meta)[lane] = meta_word;
-      if (c == 0) {
-        // header (:1674-1678; Double :1672-1680)
-        uint32_t *h = reinterpret_cast<uint32_t *>(a.out);
-        if (lane == 0) h[0] = a.dim;
-        if (lane == 1) h[1] = (uint32_t)a.n;
-        if (lane == 2) h[2] = (uint32_t)(a.n >> 32);
-        if (lane == 3) h[3] = Tr::bits;
-        if (!is64) {
-          if (lane == 4) h[4] = __float_as_uint((float)a.eb);
-          if (lane == 5) h[5] = seg;
-        } else {
-          if (lane == 4) h[4] = (uint32_t)__double_as_longlong((double)a.eb);
-          if (lane == 5) h[5] = (uint32_t)((unsigned long long)__double_as_longlong((double)a.eb) >> 32);
-          if (lane == 6) h[6] = seg;
-          if (lane == 7) h[7] = 32u;
-        }
-      }
-      if (pay_base + off + payload > a.out_cap) {
-        if (lane == 0) set_status(ctl, kENOSPACE);
-      } else {
-        copy_payload(reinterpret_cast<uint32_t *>(a.out + pay_base + off), sw, payload, lane);
-      }
-      if (c == G - 1 && lane == 0) ctl->stream_bytes = pay_base + off + payload;
-    }
+    if (c < G) payload = encode_chunk<T, DIM>(a, c, sw, seg, sh, msk, eb, inv, pts, meta_word, lane, on_size);
+    else on_size(0u);
+    if (!wait_claimed(slots[k1], it + 1, ctl)) break;
+    pts.load(a, *reinterpret_cast<volatile unsigned long long *>(&slots[k1].gbase) + warp, lane);
+    if (!place_offset(s, true, gid, a.look, ctl, lane)) break;
+    if (c < G) place_chunk<T>(a, c, G, pay_base, chunk_offset(s, warp), payload, meta_word, seg, eb, sw, lane);
+    __syncwarp();  // the staged payload is read before the region is reused
+    k = k1;
   }
   rewind_work_counter(ctl);
 }

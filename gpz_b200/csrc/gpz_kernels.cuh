@@ -178,6 +178,72 @@ __host__ __device__ SegDecision decide_seg(const T mm[6], uint32_t dim, uint32_t
   return {kOK, t, 1u};
 }
 
+// Strict-bound mode (an extension; the reference holds eb only up to the
+// rounding of its reconstruction, which its verifier hides with a 1.01*eb
+// slack, src/utils.cu:28).  Every finite point x with |x| <= M reconstructs
+// within eb when the stream is encoded with
+//   eb' = eb - u * (10 M + 4 eb),   u = 2^-24 (float) / 2^-53 (double),
+// rounded down.  With inv = fl(1/(2 eb')), nmn = fl(-m inv) (m the chunk
+// minimum, |m| <= M) and qf = fl(x inv + nmn), the computed qf is within
+// u (2 |x - m| + |m|) / (2 eb') <= 5 u M / (2 eb') of (x - m) / (2 eb'),
+// so truncation puts x within eb' + 5 u M of the center m + (2q+1) eb' of its
+// bin; the decoder's conversion of 2q+1 (< 2M/eb' + 2) to T and its final
+// fused multiply-add each add at most u (2M + eb') and u (M + 2 eb'):
+// |x - v| <= eb' + u (8 M + 3 eb') < eb.  Returns 0 when no positive eb'
+// exists.
+template <typename T>
+__host__ __device__ inline T strict_bound(T eb, T max_abs) {
+  const double u = sizeof(T) == 4 ? 5.9604644775390625e-08 : 1.1102230246251565e-16;
+  const double e = (double)eb - u * (10.0 * (double)max_abs + 4.0 * (double)eb);
+  if (!(e > 0.0)) return (T)0;
+  T r = (T)e;
+  if ((double)r > e) r = sizeof(T) == 4 ? (T)nextafterf((float)r, 0.0f) : (T)nextafter((double)r, 0.0);
+  return r;
+}
+
+// The strict bound of a snapshot (strict_bound above with M = its largest
+// coordinate magnitude, NaNs ignored), into ctl->strict_eb; kEINVAL in
+// ctl->status when there is none.  Grid-stride; the last block decides.
+template <typename T>
+__global__ void __launch_bounds__(256) strict_bound_kernel(const T *__restrict__ x, const T *__restrict__ y,
+                                                           const T *__restrict__ z, uint64_t n, uint32_t dim, T eb,
+                                                           Control *ctl) {
+  using U = typename TT<T>::U;
+  __shared__ U red[8];
+  __shared__ int last;
+  U acc = 0;
+  const T *X[3] = {x, y, z};
+  const unsigned long long step = (unsigned long long)gridDim.x * blockDim.x;
+  for (unsigned long long i = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += step)
+    for (uint32_t d = 0; d < dim; ++d) {
+      const T v = X[d][i];
+      if (v == v) acc = max(acc, ord_of(v < (T)0 ? -v : v));
+    }
+  const U w = warp_max(acc);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = w;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    U v = 0;
+    for (int k = 0; k < 8; ++k) v = max(v, red[k]);
+    atomicMax(&ctl->mm[0], (unsigned long long)v);
+  }
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) last = (atomicAdd(&ctl->sample_done, 1u) == gridDim.x - 1);
+  __syncthreads();
+  if (last && threadIdx.x == 0) {
+    __threadfence();
+    const U o = (U)((volatile unsigned long long *)ctl->mm)[0];
+    const T M = o ? from_ord(o) : (T)0;
+    const T e = strict_bound<T>(eb, M);
+    if (!(e > (T)0)) set_status(ctl, kEINVAL);
+    ctl->strict_eb = (double)e;
+    // the sampling kernel that follows reuses these accumulators
+    ctl->mm[0] = 0;
+    ctl->sample_done = 0;
+  }
+}
+
 template <typename T>
 __device__ __forceinline__ void fold_minmax(T v, typename TT<T>::U &mn_inv, typename TT<T>::U &mx) {
   if (v == v) {
@@ -199,7 +265,7 @@ template <typename T>
 __device__ __forceinline__ void seg_sample_block(const T *__restrict__ x, const T *__restrict__ y,
                                                  const T *__restrict__ z, uint64_t n, uint32_t dim, uint32_t seg_in,
                                                  int rel_mode, T rel_eb, T eb, int safe31, Control *ctl,
-                                                 unsigned block, unsigned nblocks) {
+                                                 unsigned block, unsigned nblocks, const double *eb_dev = nullptr) {
   using U = typename TT<T>::U;
   __shared__ U red[6][8];
   __shared__ int last;
@@ -246,7 +312,8 @@ __device__ __forceinline__ void seg_sample_block(const T *__restrict__ x, const 
         mm[3 + d] = 0;
       }
     }
-    const SegDecision sd = decide_seg<T>(mm, dim, seg_in, rel_mode, rel_eb, eb, safe31);
+    const T ebv = eb_dev ? (T)*(const volatile double *)eb_dev : eb;
+    const SegDecision sd = decide_seg<T>(mm, dim, seg_in, rel_mode, rel_eb, ebv, safe31);
     if (sd.status != kOK) set_status(ctl, sd.status);
     else {
       ctl->seg = sd.seg;
@@ -259,8 +326,9 @@ template <typename T>
 __global__ void __launch_bounds__(256) seg_sample_kernel(const T *__restrict__ x, const T *__restrict__ y,
                                                          const T *__restrict__ z, uint64_t n, uint32_t dim,
                                                          uint32_t seg_in, int rel_mode, T rel_eb, T eb,
-                                                         int safe31, Control *ctl) {
-  seg_sample_block<T>(x, y, z, n, dim, seg_in, rel_mode, rel_eb, eb, safe31, ctl, blockIdx.x, gridDim.x);
+                                                         int safe31, Control *ctl, const double *eb_dev) {
+  if (eb_dev && ld_volatile(reinterpret_cast<const uint32_t *>(&ctl->status)) != 0) return;
+  seg_sample_block<T>(x, y, z, n, dim, seg_in, rel_mode, rel_eb, eb, safe31, ctl, blockIdx.x, gridDim.x, eb_dev);
 }
 
 // The sampling windows of computeSegSize restricted to one shard
@@ -392,6 +460,7 @@ struct CArgs {
   unsigned long long *look;  // one look-back word per chunk
   unsigned long long n, G;
   T eb;
+  const double *eb_dev;  // when set, the bound is read here on the device (strict-bound mode)
   uint32_t dim;
   int vec_ok;  // x, y, z all 16-byte aligned
 };

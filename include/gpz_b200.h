@@ -66,6 +66,22 @@ typedef struct gpz_params {
  * whole array (gpz_sample_minmax + gpz_decide_seg); seg_size must not be 0. */
 #define GPZ_FLAG_SEG_FIXED 2u
 
+/* Extension (not in the reference): hold the stated bound for every finite
+ * point.  The reference reconstructs v = min + (2q+1)*eb in the float type
+ * (src/cudaWarpCompress.cu:971-1007), so its rounding can put a point a few
+ * ulps past eb; its verifier hides that with a 1.01*eb slack
+ * (src/utils.cu:28).  With this flag the codec finds the snapshot's largest
+ * coordinate magnitude M on the device and encodes with
+ *   eb' = eb - u*(10*M + 4*eb)   (u = 2^-24 for float, 2^-53 for double),
+ * rounded down, which bounds every rounding of quantization and
+ * reconstruction (gpz_strict_bound computes the same value on the host).
+ * The header carries eb'; the stream stays in the reference format (any GPZ
+ * decoder reads it) but its bytes differ from the reference's.  Implies
+ * GPZ_FLAG_SAFE31.  GPZ_EINVAL (device status) when eb' would not be
+ * positive.  Costs one extra pass over the input.  gpz_compress and
+ * gpz_compress_async only (the batched and served forms ignore it). */
+#define GPZ_FLAG_STRICT_BOUND 8u
+
 /* Result of a compress / decompress call, read back from device scratch. */
 typedef struct gpz_result {
   uint64_t stream_bytes; /* compressed size (compress) */
@@ -165,6 +181,11 @@ int gpz_parse_header(const void *h_stream, uint64_t bytes, uint32_t *dim, uint64
 int gpz_rel_to_abs(uint32_t float_bits, uint32_t dim, uint64_t n, const void *d_x,
                    const void *d_y, const void *d_z, double rel, void *d_scratch,
                    uint64_t scratch_bytes, double *h_eb, double *h_minmax6, void *stream);
+
+/* The bound GPZ_FLAG_STRICT_BOUND encodes with, for a snapshot whose largest
+ * coordinate magnitude is max_abs (float_bits 32: computed in float).  No
+ * counterpart in the reference.  GPZ_EINVAL when it would not be positive. */
+int gpz_strict_bound(uint32_t float_bits, double eb, double max_abs, double *eb_strict);
 
 /* ---- allocation-free compress -------------------------------------------------
  * No counterpart in the reference (whose compress allocates with cudaMalloc on
