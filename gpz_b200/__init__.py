@@ -134,7 +134,8 @@ SIGNATURES = {
                                       ctypes.c_double, _U32, ctypes.POINTER(_U32), ctypes.POINTER(_U32)]),
     "gpz_rel_abs_from_minmax": (ctypes.c_int, [_U32, ctypes.POINTER(ctypes.c_double), ctypes.c_double,
                                                ctypes.POINTER(ctypes.c_double)]),
-    "gpz_strict_bound": (ctypes.c_int, [_U32, ctypes.c_double, ctypes.c_double, ctypes.POINTER(ctypes.c_double)]),
+    "gpz_strict_bound": (ctypes.c_int, [_U32, ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                                        ctypes.POINTER(ctypes.c_double)]),
     "gpz_batch_create": (ctypes.c_int, [ctypes.POINTER(BatchItem), _U32, ctypes.POINTER(_VP), ctypes.POINTER(_U32)]),
     "gpz_batch_launch": (ctypes.c_int, [_VP, _VP]),
     "gpz_batch_results": (ctypes.c_int, [_VP, ctypes.POINTER(Result), ctypes.POINTER(ctypes.c_double), _VP]),
@@ -155,6 +156,8 @@ SIGNATURES = {
     "gpz_selftest_lookback_timeout": (ctypes.c_int, [_U32, _VP, _U64, ctypes.POINTER(ctypes.c_int32), _VP]),
     "gpz_verify": (ctypes.c_int, [_U32, _U32, _U64, _VP, _VP, _VP, _VP, _VP, _VP, ctypes.c_double, _U32, _VP, _U64,
                                   ctypes.POINTER(VerifyResult), _VP]),
+    "gpz_verify_bound": (ctypes.c_int, [_U32, _U32, _U64, _VP, _VP, _VP, _VP, _VP, _VP, ctypes.c_double, _U32,
+                                        ctypes.c_double, _VP, _U64, ctypes.POINTER(VerifyResult), _VP]),
 }
 
 _lib = None
@@ -223,11 +226,12 @@ def make_params(n: int, dim: int, float_bits: int, eb: float, seg_size: int = 0,
                   seg_size=seg_size, flags=flags, reserved=0)
 
 
-def strict_bound(float_bits: int, eb: float, max_abs: float) -> float:
+def strict_bound(float_bits: int, eb: float, max_abs: float, max_range: float) -> float:
     """The bound GPZ_FLAG_STRICT_BOUND encodes with for a snapshot whose largest
-    coordinate magnitude is max_abs (gpz_strict_bound)."""
+    coordinate magnitude is max_abs and largest per-axis range max_range
+    (gpz_strict_bound)."""
     out = ctypes.c_double()
-    _check(lib().gpz_strict_bound(float_bits, eb, max_abs, ctypes.byref(out)), "gpz_strict_bound")
+    _check(lib().gpz_strict_bound(float_bits, eb, max_abs, max_range, ctypes.byref(out)), "gpz_strict_bound")
     return out.value
 
 
@@ -328,19 +332,22 @@ def rel_to_abs(x, y, z, rel: float, stream=None):
     return eb.value, list(mm)
 
 
-def verify(x, y, z, rx, ry, rz, eb: float, seg_size: int, stream=None) -> "VerifyResult":
+def verify(x, y, z, rx, ry, rz, eb: float, seg_size: int, stream=None, bound: float | None = None) -> "VerifyResult":
     """Per-point check of a reconstruction (stream order, as decompress
     returns it) against the original SoA tensors; eb and seg_size as in the
-    stream header."""
+    stream header, `bound` the bound the errors are checked against (default
+    eb; the stated bound for a strict-bound stream, whose header eb is below
+    it)."""
     torch = _torch()
     dim = 3 if z is not None else 2
     scratch = torch.empty(int(lib().gpz_verify_scratch_bytes()), dtype=torch.uint8, device=x.device)
     res = VerifyResult()
-    rc = lib().gpz_verify(_dtype_bits(x), dim, x.numel(), x.data_ptr(), y.data_ptr(),
-                          z.data_ptr() if dim == 3 else None, rx.data_ptr(), ry.data_ptr(),
-                          rz.data_ptr() if dim == 3 else None, float(eb), int(seg_size), scratch.data_ptr(),
-                          scratch.numel(), ctypes.byref(res), _stream_ptr(stream))
-    _check(rc, "gpz_verify")
+    rc = lib().gpz_verify_bound(_dtype_bits(x), dim, x.numel(), x.data_ptr(), y.data_ptr(),
+                                z.data_ptr() if dim == 3 else None, rx.data_ptr(), ry.data_ptr(),
+                                rz.data_ptr() if dim == 3 else None, float(eb), int(seg_size),
+                                float(eb if bound is None else bound), scratch.data_ptr(), scratch.numel(),
+                                ctypes.byref(res), _stream_ptr(stream))
+    _check(rc, "gpz_verify_bound")
     return res
 
 

@@ -51,58 +51,53 @@ __global__ void __launch_bounds__(256) batch_sample_kernel(const BItem<T> *items
                       (it.flags & kBatchSafe31) ? 1 : 0, it.a.ctl, blockIdx.x, gridDim.x);
 }
 
+struct BatchGroup {
+  uint32_t sz[kEncWarps];     // payload bytes of each warp's chunk
+  unsigned long long goff;    // stream offset of the group (~0: look-back gave up)
+  unsigned long long next;    // next global group
+  unsigned long long nmap;    // its map entry
+};
+
 // The compress loop of compress_kernel over a work list of many snapshots:
-// map[g] = snapshot << 40 | group of global group g.  Each group slot also
-// holds its map entry and its snapshot's arguments (the next group's points
-// are loaded before the current group's offset is awaited).  A snapshot whose
-// segment size could not be chosen (sampling error, status set) is skipped as
-// a whole; a group whose look-back gave up is skipped and the loop goes on
-// with the other snapshots.
+// map[g] = snapshot << 40 | group of global group g.  The arguments of the
+// current and the next group's snapshot live in shared memory (double
+// buffered: the next group's points are loaded before the current group's
+// copy-out).  A snapshot whose segment size could not be chosen (sampling
+// error, status set) is skipped as a whole.
 template <typename T, int DIM>
 __global__ void __launch_bounds__(32 * kEncWarps, GPZ_ENC_MIN_CTAS)
     compress_batch_kernel(const BItem<T> *__restrict__ items, const unsigned long long *__restrict__ map,
                           unsigned long long total, unsigned long long *claim) {
   using Tr = TT<T>;
   constexpr bool is64 = sizeof(T) == 8;
+  constexpr uint32_t FULL = 0xFFFFFFFFu;
   constexpr unsigned long long kLocal = (1ull << kBatchLocalBits) - 1;
   extern __shared__ __align__(16) uint32_t enc_smem[];
-  __shared__ EncSlot slots[3];
-  __shared__ unsigned long long smap[3];
-  __shared__ CArgs<T> args[3];
+  __shared__ BatchGroup eg;
+  __shared__ CArgs<T> args[2];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   uint32_t *const sw = enc_smem + warp * kEncWords;
-  auto claim_into = [&](int j, uint32_t seq) {  // lane 0 of one warp
+  auto claim_next = [&](int slot) {  // thread 0
     const unsigned long long g = atomicAdd(claim, 1ull);
+    eg.next = g;
     // past the end: the first snapshot's first group stands in, so the
     // prefetch below needs no condition (its loads are never used)
     const unsigned long long m = g < total ? map[g] : 0ull;
-    slots[j].gbase = g;
-    slots[j].reported = 0;
-    slots[j].owner = 0;
-    slots[j].ready = 0;
-    smap[j] = m;
-    args[j] = items[m >> kBatchLocalBits].a;
-    __threadfence_block();
-    *reinterpret_cast<volatile uint32_t *>(&slots[j].seq) = seq;
+    eg.nmap = m;
+    args[slot] = items[m >> kBatchLocalBits].a;
   };
-  Control *const ctl0 = items[0].a.ctl;  // where a batch-level wait that runs out is reported
-  if (threadIdx.x == 0) {
-    slots[1].seq = slots[2].seq = ~0u;
-    claim_into(0, 0u);
-  }
+  if (threadIdx.x == 0) claim_next(0);
   __syncthreads();
   ChunkPoints<T, DIM> pts;
-  pts.load(args[0], (smap[0] & kLocal) * kEncWarps + warp, lane);
-  int k = 0;
-  for (uint32_t it = 0;; ++it) {
-    EncSlot &s = slots[k];
-    const int k1 = k == 2 ? 0 : k + 1;
-    // a snapshot that aborts does not stop the others: no abort check here
-    if (!wait_claimed(s, it, ctl0, false)) break;
-    const unsigned long long g = *reinterpret_cast<volatile unsigned long long *>(&s.gbase);
+  pts.load(args[0], (eg.nmap & kLocal) * kEncWarps + warp, lane);
+  int slot = 0;
+  for (;;) {
+    const unsigned long long g = eg.next;
     if (g >= total) break;
-    const unsigned long long m = *reinterpret_cast<volatile unsigned long long *>(&smap[k]);
-    const CArgs<T> &a = args[k];
+    const unsigned long long m = eg.nmap;
+    __syncthreads();  // B0: everyone has the group before it is replaced
+    if (threadIdx.x == 0) claim_next(slot ^ 1);
+    const CArgs<T> &a = args[slot];
     Control *ctl = a.ctl;
     const unsigned long long G = a.G;
     const unsigned long long gid = m & kLocal, gbase = gid * kEncWarps;
@@ -113,17 +108,33 @@ __global__ void __launch_bounds__(32 * kEncWarps, GPZ_ENC_MIN_CTAS)
     const T inv = is64 ? (T)__ddiv_rn(1.0, __dmul_rn(2.0, (double)eb)) : (T)__fdiv_rn(1.0f, __fmul_rn(2.0f, (float)eb));
     const unsigned long long pay_base = Tr::hdr + 8ull * G + (unsigned long long)Tr::meta * G;
     const unsigned long long c = gbase + warp;
-    auto on_size = [&](uint32_t bytes) { report_size(s, bytes, warp, lane, [&]() { claim_into(k1, it + 1); }); };
+    uint32_t tot = 0;
+    auto on_size = [&](uint32_t bytes) {
+      if (lane == 0) eg.sz[warp] = bytes;
+      __syncthreads();  // B1: the group's sizes are known (and the next group's snapshot)
+      if (live && warp == 0) {
+        const uint32_t s = lane < kEncWarps ? eg.sz[lane] : 0u;
+        tot = __reduce_add_sync(FULL, s);
+        if (lane == 0) publish_aggregate(a.look, gid, tot);
+      }
+    };
     uint32_t payload = 0, meta_word = 0;
     if (live && c < G) payload = encode_chunk<T, DIM>(a, c, sw, seg, sh, msk, eb, inv, pts, meta_word, lane, on_size);
     else on_size(0u);
-    if (!wait_claimed(slots[k1], it + 1, ctl0, false)) break;
-    pts.load(args[k1], (*reinterpret_cast<volatile unsigned long long *>(&smap[k1]) & kLocal) * kEncWarps + warp,
-             lane);
-    if (place_offset(s, live, gid, a.look, ctl, lane) && c < G)
-      place_chunk<T>(a, c, G, pay_base, chunk_offset(s, warp), payload, meta_word, seg, eb, sw, lane);
-    __syncwarp();  // the staged payload is read before the region is reused
-    k = k1;
+    if (live && warp == 0) {
+      unsigned long long excl = 0;
+      const bool ok = resolve_prefix(a.look, gid, tot, ctl, excl);
+      if (lane == 0) eg.goff = ok ? excl : ~0ull;
+    }
+    pts.load(args[slot ^ 1], (eg.nmap & kLocal) * kEncWarps + warp, lane);  // in flight during the copy-out
+    __syncthreads();  // B2: the group's stream offset is known
+    const unsigned long long goff = eg.goff;
+    if (live && c < G && goff != ~0ull) {
+      unsigned long long off = goff;
+      for (int w = 0; w < warp; ++w) off += eg.sz[w];
+      place_chunk<T>(a, c, G, pay_base, off, payload, meta_word, seg, eb, sw, lane);
+    }
+    slot ^= 1;
   }
 }
 

@@ -402,10 +402,12 @@ int gpz_decide_seg(uint32_t float_bits, uint32_t dim, const uint64_t *acc6, uint
   return GPZ_OK;
 }
 
-int gpz_strict_bound(uint32_t float_bits, double eb, double max_abs, double *eb_strict) {
-  if ((float_bits != 32 && float_bits != 64) || !eb_strict || !(eb > 0.0) || !(max_abs >= 0.0)) return GPZ_EINVAL;
-  const double e = float_bits == 32 ? (double)strict_bound<float>((float)eb, (float)max_abs)
-                                    : strict_bound<double>(eb, max_abs);
+int gpz_strict_bound(uint32_t float_bits, double eb, double max_abs, double max_range, double *eb_strict) {
+  if ((float_bits != 32 && float_bits != 64) || !eb_strict || !(eb > 0.0) || !(max_abs >= 0.0) ||
+      !(max_range >= 0.0))
+    return GPZ_EINVAL;
+  const double e = float_bits == 32 ? (double)strict_bound<float>((float)eb, max_abs, max_range)
+                                    : strict_bound<double>(eb, max_abs, max_range);
   if (!(e > 0.0)) return GPZ_EINVAL;
   *eb_strict = e;
   return GPZ_OK;

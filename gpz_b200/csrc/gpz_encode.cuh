@@ -47,18 +47,11 @@ constexpr int kEncSmall = 16;             // buckets of this many points or more
 constexpr int kEncWords = 3 * kChunk;     // per-warp shared words (12 KB)
 static_assert(kStageBytes <= kEncWords * 4, "payload staging must fit the warp region");
 
-// Per-CTA state of one group of kEncWarps consecutive chunks.  Three slots
-// rotate: the group being encoded, the next one (claimed by the first warp to
-// report a size in the current one) and the previous one (still being copied
-// out by slower warps).
-struct EncSlot {
-  unsigned long long gbase;  // first chunk of the group (>= G: no more work)
-  uint32_t seq;              // loop iteration whose group the slot holds (set last by the claimer)
-  unsigned long long goff;   // stream offset of the group's payloads (~0: the look-back gave up)
+// Per-CTA state of the group of kEncWarps consecutive chunks a CTA encodes.
+struct EncGroup {
   uint32_t sz[kEncWarps];    // payload bytes of each warp's chunk
-  uint32_t reported;         // warps whose size is in sz
-  uint32_t owner;            // set by the warp that resolves the group's offset
-  uint32_t ready;            // goff is final
+  unsigned long long goff;   // stream offset of the group (~0: look-back gave up)
+  unsigned long long next;   // first chunk of the next group
 };
 
 constexpr size_t enc_smem_bytes() { return (size_t)kEncWarps * kEncWords * 4; }
@@ -853,111 +846,6 @@ __device__ __forceinline__ void copy_payload(uint32_t *dst, const uint32_t *sw, 
   }
 }
 
-// Group bookkeeping shared by the plain and batched compress kernels.
-//
-// report_size: this warp's payload size for the group in slot s, reported as
-// soon as it is known (before the bit planes are built).  The first warp of
-// the CTA to report claims the next group (claim_next(), lane 0): it fills
-// the slot of the group before the previous one, which no warp uses any more
-// (a warp enters a group only after every warp has reported in the group
-// before it), and sets the slot's seq last.  Warp-collective.
-template <class ClaimNext>
-__device__ __forceinline__ void report_size(EncSlot &s, uint32_t bytes, int warp, int lane, ClaimNext &&claim_next) {
-  if (lane == 0) {
-    s.sz[warp] = bytes;
-    __threadfence_block();
-    if (atomicAdd(&s.reported, 1u) == 0u) claim_next();
-  }
-  __syncwarp();
-}
-
-// Waits (bounded) until slot s holds the group of loop iteration `seq`; a
-// wait that runs out (or, with check_abort, another CTA's abort) is reported
-// in ctl.
-__device__ __forceinline__ bool wait_claimed(const EncSlot &s, uint32_t seq, Control *ctl, bool check_abort = true) {
-  uint32_t spins = 0;
-  while (ld_volatile(&s.seq) != seq) {
-    if (++spins > 4u * kSpinLimit || (check_abort && (spins & 63u) == 0u && ld_volatile(&ctl->abort))) {
-      if ((threadIdx.x & 31) == 0) {
-        atomicExch(&ctl->abort, 1u);
-        set_status(ctl, kETIMEOUT);
-      }
-      return false;
-    }
-    __nanosleep(64);
-  }
-  __threadfence_block();
-  return true;
-}
-
-// place_offset: the group's stream offset, once this warp's payload is staged.
-// The first warp to get here owns the group: it waits (bounded) for the other
-// warps' sizes, publishes the group's aggregate, resolves its offset by
-// decoupled look-back (bounded; skipped when !live) and releases it.  The
-// others wait (bounded) for it.  So the look-back runs on a warp that has
-// nothing else to do, while slower warps still build their planes.  Returns
-// false when the group is not placed (look-back gave up, another CTA aborted,
-// or a wait ran out).  Warp-collective.
-__device__ __forceinline__ bool place_offset(EncSlot &s, bool live, unsigned long long gid, unsigned long long *look,
-                                             Control *ctl, int lane) {
-  constexpr uint32_t FULL = 0xFFFFFFFFu;
-  uint32_t own = 0;
-  if (lane == 0) own = atomicCAS(&s.owner, 0u, 1u) == 0u;
-  own = __shfl_sync(FULL, own, 0);
-  auto give_up = [&]() {
-    if (lane == 0) {
-      atomicExch(&ctl->abort, 1u);
-      set_status(ctl, kETIMEOUT);
-    }
-  };
-  if (own) {
-    uint32_t spins = 0, backoff = 32;
-    bool ok = true;
-    while (ld_volatile(&s.reported) < (uint32_t)kEncWarps) {
-      if (++spins > 2u * kSpinLimit || ((spins & 63u) == 0u && ld_volatile(&ctl->abort))) {
-        give_up();
-        ok = false;
-        break;
-      }
-      __nanosleep(backoff);
-      backoff = min(backoff * 2, 256u);
-    }
-    __threadfence_block();
-    unsigned long long excl = 0;
-    if (ok && live) {
-      const uint32_t v = lane < kEncWarps ? ld_volatile(&s.sz[lane]) : 0u;
-      const uint32_t total = __reduce_add_sync(FULL, v);
-      if (lane == 0) publish_aggregate(look, gid, total);
-      ok = resolve_prefix(look, gid, total, ctl, excl);
-    }
-    if (lane == 0) {
-      s.goff = ok && live ? excl : ~0ull;
-      __threadfence_block();
-      *reinterpret_cast<volatile uint32_t *>(&s.ready) = 1u;
-    }
-    __syncwarp();
-    return ok && live;
-  }
-  uint32_t spins = 0, backoff = 32;
-  while (ld_volatile(&s.ready) == 0u) {
-    if (++spins > 4u * kSpinLimit || ((spins & 63u) == 0u && ld_volatile(&ctl->abort))) {
-      give_up();
-      return false;
-    }
-    __nanosleep(backoff);
-    backoff = min(backoff * 2, 256u);
-  }
-  __threadfence_block();
-  return *reinterpret_cast<const volatile unsigned long long *>(&s.goff) != ~0ull;
-}
-
-// Stream offset of warp w's chunk in a placed group.
-__device__ __forceinline__ unsigned long long chunk_offset(const EncSlot &s, int warp) {
-  unsigned long long off = *reinterpret_cast<const volatile unsigned long long *>(&s.goff);
-  for (int w = 0; w < warp; ++w) off += ld_volatile(&s.sz[w]);
-  return off;
-}
-
 // Writes a placed chunk: its offset-table entry (:1679), meta record, payload,
 // and for chunk 0 the header (:1674-1678; Double :1672-1680).
 template <typename T>
@@ -994,17 +882,19 @@ __device__ __forceinline__ void place_chunk(const CArgs<T> &a, unsigned long lon
 }
 
 // Persistent compress kernel: every CTA encodes groups of kEncWarps
-// consecutive chunks, one chunk per warp.  No CTA-wide barrier inside the
-// loop: a warp reports its payload size as soon as it is known, the last
-// reporter resolves the group's offset while the others build their bit
-// planes, and each warp then waits only for that offset before copying its
-// staged payload out.  Warps of a CTA are at most one group apart.
+// consecutive chunks, one chunk per warp.  Per group: the warps quantize,
+// rank and find the runs of their chunks; their payload sizes are then known
+// (barrier B1) and warp 0 publishes the group's aggregate, so that later
+// groups' look-backs can pass it while the warps build their bit planes;
+// warp 0 then resolves the group's stream offset (decoupled look-back) and
+// after barrier B2 every warp copies its staged payload out.
 template <typename T, int DIM>
 __global__ void __launch_bounds__(32 * kEncWarps, GPZ_ENC_MIN_CTAS) compress_kernel(const CArgs<T> a) {
   using Tr = TT<T>;
   constexpr bool is64 = sizeof(T) == 8;
+  constexpr uint32_t FULL = 0xFFFFFFFFu;
   extern __shared__ __align__(16) uint32_t enc_smem[];
-  __shared__ EncSlot slots[3];
+  __shared__ EncGroup eg;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   uint32_t *const sw = enc_smem + warp * kEncWords;
   Control *ctl = a.ctl;
@@ -1015,39 +905,46 @@ __global__ void __launch_bounds__(32 * kEncWarps, GPZ_ENC_MIN_CTAS) compress_ker
   const T inv = is64 ? (T)__ddiv_rn(1.0, __dmul_rn(2.0, (double)eb)) : (T)__fdiv_rn(1.0f, __fmul_rn(2.0f, (float)eb));
   const unsigned long long G = a.G;
   const unsigned long long pay_base = Tr::hdr + 8ull * G + (unsigned long long)Tr::meta * G;
-  auto claim_into = [&](EncSlot &t, uint32_t seq) {  // lane 0 of one warp
-    t.gbase = ld_volatile(&ctl->abort) ? G : (unsigned long long)atomicAdd(&ctl->chunk_ctr, (uint32_t)kEncWarps);
-    t.reported = 0;
-    t.owner = 0;
-    t.ready = 0;
-    __threadfence_block();
-    *reinterpret_cast<volatile uint32_t *>(&t.seq) = seq;
-  };
-  if (threadIdx.x == 0) {
-    slots[1].seq = slots[2].seq = ~0u;
-    claim_into(slots[0], 0u);
-  }
+
+  if (threadIdx.x == 0) eg.next = atomicAdd(&ctl->chunk_ctr, (uint32_t)kEncWarps);
   __syncthreads();
   ChunkPoints<T, DIM> pts;
-  pts.load(a, slots[0].gbase + warp, lane);
-  int k = 0;
-  for (uint32_t it = 0;; ++it) {
-    EncSlot &s = slots[k];
-    const int k1 = k == 2 ? 0 : k + 1;
-    if (!wait_claimed(s, it, ctl)) break;
-    const unsigned long long gbase = *reinterpret_cast<volatile unsigned long long *>(&s.gbase);
+  pts.load(a, eg.next + warp, lane);
+  for (;;) {
+    const unsigned long long gbase = eg.next;
     if (gbase >= G) break;
-    const unsigned long long c = gbase + warp, gid = gbase / kEncWarps;
-    auto on_size = [&](uint32_t bytes) { report_size(s, bytes, warp, lane, [&]() { claim_into(slots[k1], it + 1); }); };
+    __syncthreads();  // B0: everyone has the group before it is replaced
+    if (threadIdx.x == 0) eg.next = ld_volatile(&ctl->abort) ? G : atomicAdd(&ctl->chunk_ctr, (uint32_t)kEncWarps);
+    const unsigned long long c = gbase + warp;
+    const unsigned long long gid = gbase / kEncWarps;
+    uint32_t total = 0;
+    auto on_size = [&](uint32_t bytes) {
+      if (lane == 0) eg.sz[warp] = bytes;
+      __syncthreads();  // B1: the group's sizes are known
+      if (warp == 0) {
+        const uint32_t s = lane < kEncWarps ? eg.sz[lane] : 0u;
+        total = __reduce_add_sync(FULL, s);
+        if (lane == 0) publish_aggregate(a.look, gid, total);
+      }
+    };
     uint32_t payload = 0, meta_word = 0;
     if (c < G) payload = encode_chunk<T, DIM>(a, c, sw, seg, sh, msk, eb, inv, pts, meta_word, lane, on_size);
     else on_size(0u);
-    if (!wait_claimed(slots[k1], it + 1, ctl)) break;
-    pts.load(a, *reinterpret_cast<volatile unsigned long long *>(&slots[k1].gbase) + warp, lane);
-    if (!place_offset(s, true, gid, a.look, ctl, lane)) break;
-    if (c < G) place_chunk<T>(a, c, G, pay_base, chunk_offset(s, warp), payload, meta_word, seg, eb, sw, lane);
-    __syncwarp();  // the staged payload is read before the region is reused
-    k = k1;
+    if (warp == 0) {
+      // resolved only now: the predecessors have had this group's plane
+      // building to publish, so the look-back rarely waits
+      unsigned long long excl = 0;
+      const bool ok = resolve_prefix(a.look, gid, total, ctl, excl);
+      if (lane == 0) eg.goff = ok ? excl : ~0ull;
+    }
+    pts.load(a, eg.next + warp, lane);  // in flight during the copy-out
+    __syncthreads();  // B2: the group's stream offset is known
+    const unsigned long long goff = eg.goff;
+    if (c < G && goff != ~0ull) {
+      unsigned long long off = goff;
+      for (int w = 0; w < warp; ++w) off += eg.sz[w];
+      place_chunk<T>(a, c, G, pay_base, off, payload, meta_word, seg, eb, sw, lane);
+    }
   }
   rewind_work_counter(ctl);
 }

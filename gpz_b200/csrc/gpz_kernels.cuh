@@ -178,54 +178,67 @@ __host__ __device__ SegDecision decide_seg(const T mm[6], uint32_t dim, uint32_t
   return {kOK, t, 1u};
 }
 
+template <typename T>
+__device__ __forceinline__ void fold_minmax(T v, typename TT<T>::U &mn_inv, typename TT<T>::U &mx) {
+  if (v == v) {
+    const typename TT<T>::U o = ord_of(v);
+    mn_inv = max(mn_inv, (typename TT<T>::U)~o);
+    mx = max(mx, o);
+  }
+}
+
 // Strict-bound mode (an extension; the reference holds eb only up to the
 // rounding of its reconstruction, which its verifier hides with a 1.01*eb
-// slack, src/utils.cu:28).  Every finite point x with |x| <= M reconstructs
+// slack, src/utils.cu:28).  For a snapshot whose coordinates satisfy |x| <= M
+// and whose per-axis ranges are at most R, every finite point reconstructs
 // within eb when the stream is encoded with
-//   eb' = eb - u * (10 M + 4 eb),   u = 2^-24 (float) / 2^-53 (double),
-// rounded down.  With inv = fl(1/(2 eb')), nmn = fl(-m inv) (m the chunk
-// minimum, |m| <= M) and qf = fl(x inv + nmn), the computed qf is within
-// u (2 |x - m| + |m|) / (2 eb') <= 5 u M / (2 eb') of (x - m) / (2 eb'),
-// so truncation puts x within eb' + 5 u M of the center m + (2q+1) eb' of its
-// bin; the decoder's conversion of 2q+1 (< 2M/eb' + 2) to T and its final
-// fused multiply-add each add at most u (2M + eb') and u (M + 2 eb'):
-// |x - v| <= eb' + u (8 M + 3 eb') < eb.  Returns 0 when no positive eb'
-// exists.
+//   eb' = eb - u * (3 R + 2 M + 4 eb),   u = 2^-24 (float) / 2^-53 (double),
+// rounded down.  With t = (x - m) / (2 eb') (m the chunk minimum, 0 <= x - m
+// <= R), inv = fl(1/(2 eb')) = (1 + d1) / (2 eb'), nmn = fl(-m inv) and
+// qf = fl(x inv + nmn), |qf - t| <= u (2 t + |m| inv) + O(u^2): truncation
+// leaves x within eb' + u (2R + M) of the center m + (2q+1) eb' of its bin.
+// The decoder's fused multiply-add rounds the center once, by at most
+// u (M + eb'), and its conversion of 2q+1 (<= R/eb' + 1) to T by at most
+// u (R + eb') eb'/eb' when 2q+1 needs more than the mantissa:
+//   |x - v| <= eb' + u (3R + 2M + 2 eb') + O(u^2) < eb.
+// Returns 0 when no positive eb' exists.
 template <typename T>
-__host__ __device__ inline T strict_bound(T eb, T max_abs) {
+__host__ __device__ inline T strict_bound(T eb, double max_abs, double max_range) {
   const double u = sizeof(T) == 4 ? 5.9604644775390625e-08 : 1.1102230246251565e-16;
-  const double e = (double)eb - u * (10.0 * (double)max_abs + 4.0 * (double)eb);
+  const double e = (double)eb - u * (3.0 * max_range + 2.0 * max_abs + 4.0 * (double)eb);
   if (!(e > 0.0)) return (T)0;
   T r = (T)e;
   if ((double)r > e) r = sizeof(T) == 4 ? (T)nextafterf((float)r, 0.0f) : (T)nextafter((double)r, 0.0);
   return r;
 }
 
-// The strict bound of a snapshot (strict_bound above with M = its largest
-// coordinate magnitude, NaNs ignored), into ctl->strict_eb; kEINVAL in
-// ctl->status when there is none.  Grid-stride; the last block decides.
+// The strict bound of a snapshot (strict_bound above with its largest
+// coordinate magnitude and largest per-axis range, NaNs ignored), into
+// ctl->strict_eb; kEINVAL in ctl->status when there is none.  Grid-stride;
+// the last block decides.
 template <typename T>
 __global__ void __launch_bounds__(256) strict_bound_kernel(const T *__restrict__ x, const T *__restrict__ y,
                                                            const T *__restrict__ z, uint64_t n, uint32_t dim, T eb,
                                                            Control *ctl) {
   using U = typename TT<T>::U;
-  __shared__ U red[8];
+  __shared__ U red[6][8];
   __shared__ int last;
-  U acc = 0;
+  U acc[6] = {0, 0, 0, 0, 0, 0};  // [min_inv, max] per axis
   const T *X[3] = {x, y, z};
   const unsigned long long step = (unsigned long long)gridDim.x * blockDim.x;
   for (unsigned long long i = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += step)
-    for (uint32_t d = 0; d < dim; ++d) {
-      const T v = X[d][i];
-      if (v == v) acc = max(acc, ord_of(v < (T)0 ? -v : v));
-    }
-  const U w = warp_max(acc);
-  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = w;
+    for (uint32_t d = 0; d < dim; ++d) fold_minmax<T>(X[d][i], acc[2 * d], acc[2 * d + 1]);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int k = 0; k < 6; ++k) {
+    const U v = warp_max(acc[k]);
+    if (lane == 0) red[k][warp] = v;
+  }
   __syncthreads();
-  if (threadIdx.x == 0) {
+  if (threadIdx.x < 2 * dim) {
     U v = 0;
-    for (int k = 0; k < 8; ++k) v = max(v, red[k]);
-    atomicMax(&ctl->mm[0], (unsigned long long)v);
+    for (int w = 0; w < 8; ++w) v = max(v, red[threadIdx.x][w]);
+    atomicMax(&ctl->mm[threadIdx.x], (unsigned long long)v);
   }
   __threadfence();
   __syncthreads();
@@ -233,23 +246,21 @@ __global__ void __launch_bounds__(256) strict_bound_kernel(const T *__restrict__
   __syncthreads();
   if (last && threadIdx.x == 0) {
     __threadfence();
-    const U o = (U)((volatile unsigned long long *)ctl->mm)[0];
-    const T M = o ? from_ord(o) : (T)0;
-    const T e = strict_bound<T>(eb, M);
+    double M = 0.0, R = 0.0;
+    for (uint32_t d = 0; d < dim; ++d) {
+      const U mi = (U)~(U)((volatile unsigned long long *)ctl->mm)[2 * d];
+      const U ma = (U)((volatile unsigned long long *)ctl->mm)[2 * d + 1];
+      if (ma == 0) continue;  // no finite value on this axis
+      const double lo = (double)from_ord(mi), hi = (double)from_ord(ma);
+      M = fmax(M, fmax(fabs(lo), fabs(hi)));
+      R = fmax(R, hi - lo);
+    }
+    const T e = strict_bound<T>(eb, M, R);
     if (!(e > (T)0)) set_status(ctl, kEINVAL);
     ctl->strict_eb = (double)e;
     // the sampling kernel that follows reuses these accumulators
-    ctl->mm[0] = 0;
+    for (int k = 0; k < 6; ++k) ctl->mm[k] = 0;
     ctl->sample_done = 0;
-  }
-}
-
-template <typename T>
-__device__ __forceinline__ void fold_minmax(T v, typename TT<T>::U &mn_inv, typename TT<T>::U &mx) {
-  if (v == v) {
-    const typename TT<T>::U o = ord_of(v);
-    mn_inv = max(mn_inv, (typename TT<T>::U)~o);
-    mx = max(mx, o);
   }
 }
 

@@ -42,7 +42,7 @@ __global__ void __launch_bounds__(32 * kVerifyWarps) verify_kernel(const T *__re
                                                                    const T *__restrict__ z, const T *__restrict__ rx,
                                                                    const T *__restrict__ ry, const T *__restrict__ rz,
                                                                    unsigned long long n, T eb, uint32_t seg,
-                                                                   VerifyAcc *acc) {
+                                                                   T bound, VerifyAcc *acc) {
   using UO = typename TT<T>::U;
   constexpr bool is64 = sizeof(T) == 8;
   constexpr uint32_t FULL = 0xFFFFFFFFu;
@@ -56,7 +56,7 @@ __global__ void __launch_bounds__(32 * kVerifyWarps) verify_kernel(const T *__re
   const T inv = is64 ? (T)__ddiv_rn(1.0, __dmul_rn(2.0, (double)eb)) : (T)__fdiv_rn(1.0f, __fmul_rn(2.0f, (float)eb));
   const unsigned long long G = (n + kChunk - 1) / kChunk;
   unsigned long long over = 0, over_tol = 0;
-  const T tol = (T)1.01f * eb;
+  const T tol = (T)1.01f * bound;
   T emax[3] = {0, 0, 0};
   double sq[3] = {0.0, 0.0, 0.0};
   UO gmn[3] = {0, 0, 0}, gmx[3] = {0, 0, 0};
@@ -140,7 +140,7 @@ __global__ void __launch_bounds__(32 * kVerifyWarps) verify_kernel(const T *__re
       for (int d = 0; d < DIM; ++d) {
         const T o = X[d][base + p], rec = R[d][base + s];
         const T e = o > rec ? o - rec : rec - o;
-        off |= !(e <= eb);
+        off |= !(e <= bound);
         off_tol |= !(e <= tol);
         emax[d] = fmax(emax[d], e);
         sq[d] += (double)e * (double)e;
@@ -181,7 +181,8 @@ double unord(unsigned long long o) {
 
 template <typename T>
 int verify_t(uint32_t dim, uint64_t n, const void *dx, const void *dy, const void *dz, const void *rx, const void *ry,
-             const void *rz, double eb, uint32_t seg, void *d_scratch, gpz_verify_result *out, cudaStream_t st) {
+             const void *rz, double eb, uint32_t seg, double bound, void *d_scratch, gpz_verify_result *out,
+             cudaStream_t st) {
   VerifyAcc *acc = static_cast<VerifyAcc *>(d_scratch);
   if (cudaMemsetAsync(acc, 0, sizeof(VerifyAcc), st) != cudaSuccess) return GPZ_ECUDA;
   const size_t smem = (size_t)kVerifyWarps * kChunk * 8;
@@ -193,7 +194,7 @@ int verify_t(uint32_t dim, uint64_t n, const void *dx, const void *dy, const voi
     const int occ = resident_ctas(kernel, 32 * kVerifyWarps, smem);
     if (occ == 0) return false;
     const uint64_t grid = std::min<uint64_t>((G + kVerifyWarps - 1) / kVerifyWarps, (uint64_t)sms * occ);
-    kernel<<<(unsigned)grid, 32 * kVerifyWarps, smem, st>>>(x, y, z, a, b, c, n, (T)eb, seg, acc);
+    kernel<<<(unsigned)grid, 32 * kVerifyWarps, smem, st>>>(x, y, z, a, b, c, n, (T)eb, seg, (T)bound, acc);
     return true;
   };
   if (!(dim == 3 ? launch(verify_kernel<T, 3>) : launch(verify_kernel<T, 2>))) return GPZ_ECUDA;
@@ -227,18 +228,25 @@ extern "C" {
 
 uint64_t gpz_verify_scratch_bytes(void) { return 256; }
 
-int gpz_verify(uint32_t float_bits, uint32_t dim, uint64_t n, const void *d_x, const void *d_y, const void *d_z,
-               const void *d_rx, const void *d_ry, const void *d_rz, double eb, uint32_t seg_size, void *d_scratch,
-               uint64_t scratch_bytes, gpz_verify_result *result, void *stream) {
+int gpz_verify_bound(uint32_t float_bits, uint32_t dim, uint64_t n, const void *d_x, const void *d_y, const void *d_z,
+                     const void *d_rx, const void *d_ry, const void *d_rz, double eb, uint32_t seg_size, double bound,
+                     void *d_scratch, uint64_t scratch_bytes, gpz_verify_result *result, void *stream) {
   if ((float_bits != 32 && float_bits != 64) || (dim != 2 && dim != 3) || n == 0 || !d_x || !d_y ||
-      (dim == 3 && !d_z) || !d_rx || !d_ry || (dim == 3 && !d_rz) || seg_size == 0 || !(eb > 0.0) || !d_scratch ||
-      !result)
+      (dim == 3 && !d_z) || !d_rx || !d_ry || (dim == 3 && !d_rz) || seg_size == 0 || !(eb > 0.0) ||
+      !(bound > 0.0) || !d_scratch || !result)
     return GPZ_EINVAL;
   if (scratch_bytes < sizeof(VerifyAcc)) return GPZ_ENOSPACE;
   cudaStream_t st = static_cast<cudaStream_t>(stream);
-  return float_bits == 32 ? verify_t<float>(dim, n, d_x, d_y, d_z, d_rx, d_ry, d_rz, eb, seg_size, d_scratch, result, st)
-                          : verify_t<double>(dim, n, d_x, d_y, d_z, d_rx, d_ry, d_rz, eb, seg_size, d_scratch, result,
-                                             st);
+  return float_bits == 32
+             ? verify_t<float>(dim, n, d_x, d_y, d_z, d_rx, d_ry, d_rz, eb, seg_size, bound, d_scratch, result, st)
+             : verify_t<double>(dim, n, d_x, d_y, d_z, d_rx, d_ry, d_rz, eb, seg_size, bound, d_scratch, result, st);
+}
+
+int gpz_verify(uint32_t float_bits, uint32_t dim, uint64_t n, const void *d_x, const void *d_y, const void *d_z,
+               const void *d_rx, const void *d_ry, const void *d_rz, double eb, uint32_t seg_size, void *d_scratch,
+               uint64_t scratch_bytes, gpz_verify_result *result, void *stream) {
+  return gpz_verify_bound(float_bits, dim, n, d_x, d_y, d_z, d_rx, d_ry, d_rz, eb, seg_size, eb, d_scratch,
+                          scratch_bytes, result, stream);
 }
 
 }  // extern "C"

@@ -71,8 +71,9 @@ typedef struct gpz_params {
  * (src/cudaWarpCompress.cu:971-1007), so its rounding can put a point a few
  * ulps past eb; its verifier hides that with a 1.01*eb slack
  * (src/utils.cu:28).  With this flag the codec finds the snapshot's largest
- * coordinate magnitude M on the device and encodes with
- *   eb' = eb - u*(10*M + 4*eb)   (u = 2^-24 for float, 2^-53 for double),
+ * coordinate magnitude M and largest per-axis range R on the device and
+ * encodes with
+ *   eb' = eb - u*(3*R + 2*M + 4*eb)   (u = 2^-24 for float, 2^-53 for double),
  * rounded down, which bounds every rounding of quantization and
  * reconstruction (gpz_strict_bound computes the same value on the host).
  * The header carries eb'; the stream stays in the reference format (any GPZ
@@ -183,9 +184,10 @@ int gpz_rel_to_abs(uint32_t float_bits, uint32_t dim, uint64_t n, const void *d_
                    uint64_t scratch_bytes, double *h_eb, double *h_minmax6, void *stream);
 
 /* The bound GPZ_FLAG_STRICT_BOUND encodes with, for a snapshot whose largest
- * coordinate magnitude is max_abs (float_bits 32: computed in float).  No
- * counterpart in the reference.  GPZ_EINVAL when it would not be positive. */
-int gpz_strict_bound(uint32_t float_bits, double eb, double max_abs, double *eb_strict);
+ * coordinate magnitude is max_abs and whose largest per-axis range
+ * (max - min) is max_range.  No counterpart in the reference.  GPZ_EINVAL
+ * when it would not be positive. */
+int gpz_strict_bound(uint32_t float_bits, double eb, double max_abs, double max_range, double *eb_strict);
 
 /* ---- allocation-free compress -------------------------------------------------
  * No counterpart in the reference (whose compress allocates with cudaMalloc on
@@ -448,6 +450,16 @@ uint64_t gpz_verify_scratch_bytes(void);
 int gpz_verify(uint32_t float_bits, uint32_t dim, uint64_t n, const void *d_x, const void *d_y, const void *d_z,
                const void *d_rx, const void *d_ry, const void *d_rz, double eb, uint32_t seg_size, void *d_scratch,
                uint64_t scratch_bytes, gpz_verify_result *result, void *stream);
+
+/* gpz_verify with the pairing and the check apart: `eb` and seg_size are the
+ * stream's (its header), `bound` the error bound the points are checked
+ * against (over_bound counts errors above bound, over_bound_tol above
+ * 1.01*bound).  For streams encoded in strict-bound mode, whose header
+ * carries a bound below the stated one.  No counterpart in the reference. */
+int gpz_verify_bound(uint32_t float_bits, uint32_t dim, uint64_t n, const void *d_x, const void *d_y,
+                     const void *d_z, const void *d_rx, const void *d_ry, const void *d_rz, double eb,
+                     uint32_t seg_size, double bound, void *d_scratch, uint64_t scratch_bytes,
+                     gpz_verify_result *result, void *stream);
 
 /* ---- self-test of the bounded waits ---------------------------------------------
  * No counterpart in the reference (its placement is a separate CUB scan, with

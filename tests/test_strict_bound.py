@@ -4,8 +4,9 @@ reconstructs within the stated bound.
 The reference reconstructs min + (2q+1)*eb in the float type
 (src/cudaWarpCompress.cu:971-1007), so points can land a few ulps past eb;
 its verifier tolerates 1.01*eb (src/utils.cu:28).  In strict mode the codec
-encodes with eb' = eb - u*(10*M + 4*eb) (M = largest coordinate magnitude,
-u = 2^-24 / 2^-53), computed on the device; the stream is an ordinary GPZ
+encodes with eb' = eb - u*(3*R + 2*M + 4*eb) (M = largest coordinate
+magnitude, R = largest per-axis range, u = 2^-24 / 2^-53), computed on the
+device; the stream is an ordinary GPZ
 stream whose header carries eb', so the CPU oracle given eb' must produce the
 same bytes.
 """
@@ -20,15 +21,15 @@ import gpz_b200 as gz  # noqa: E402
 
 
 def test_strict_bound_host_formula():
-    """gpz_strict_bound: eb' = eb - u*(10M + 4eb), rounded down to the float type."""
-    e = gz.strict_bound(32, 0.1, 1000.0)
+    """gpz_strict_bound: eb' = eb - u*(3R + 2M + 4eb), rounded down to the float type."""
+    e = gz.strict_bound(32, 0.1, 1000.0, 999.0)
     assert e < np.float32(0.1) and e == float(np.float32(e))
-    assert 0.1 - e >= 2.0 ** -24 * (10 * 1000.0 + 0.4) * 0.999
-    assert 0.1 - e < 2.0 ** -24 * (10 * 1000.0 + 0.4) * 1.01 + 1e-8
-    e64 = gz.strict_bound(64, 1e-5, 369.0)
-    assert 1e-5 - e64 >= 2.0 ** -53 * (3690.0) and e64 > 0
+    m = 2.0 ** -24 * (3 * 999.0 + 2 * 1000.0 + 0.4)
+    assert m <= 0.1 - e < m + 1e-8
+    e64 = gz.strict_bound(64, 1e-5, 369.0, 368.0)
+    assert 1e-5 - e64 >= 2.0 ** -53 * (3 * 368.0 + 2 * 369.0) and e64 > 0
     with pytest.raises(gz.GpzError):
-        gz.strict_bound(32, 1e-6, 1e6)  # no positive bound is left
+        gz.strict_bound(32, 1e-6, 1e6, 1e6)  # no positive bound is left
 
 
 CASES = [
@@ -58,8 +59,10 @@ def test_strict_mode_holds_the_bound_and_matches_the_oracle(case):
     assert r.status == 0
     host = s.cpu().numpy().tobytes()
     hdr = gz.parse_header(host[:32])
-    M = max(float(np.nanmax(np.abs(a))) for a in ((x, y, z) if dim == 3 else (x, y)))
-    eb_s = gz.strict_bound(bits, eb, M)
+    axes = (x, y, z) if dim == 3 else (x, y)
+    M = max(float(np.nanmax(np.abs(a))) for a in axes)
+    R = max(float(np.nanmax(a)) - float(np.nanmin(a)) for a in axes)
+    eb_s = gz.strict_bound(bits, eb, M, R)
     assert hdr["eb"] == eb_s < eb
     # the same stream from the oracle given eb' (SAFE31 rules for the segment size)
     seg, adj = po.seg_size(x, y, z, dim, seg_in, mode == "rel", typed(e), eb_s, True)
@@ -67,7 +70,7 @@ def test_strict_mode_holds_the_bound_and_matches_the_oracle(case):
     assert host == po.compress(x, y, z, dim, eb_s, seg)
     # every point within the stated bound
     dx, dy, dz = gz.decompress(s)
-    v = gz.verify(tx, ty, tz, dx, dy, dz, eb, r.seg_size)
+    v = gz.verify(tx, ty, tz, dx, dy, dz, eb_s, r.seg_size, bound=eb)
     assert v.over_bound == 0 and v.over_bound_tol == 0, (v.over_bound, list(v.max_abs_err))
     assert max(v.max_abs_err[:dim]) <= eb
 
@@ -86,5 +89,6 @@ def test_default_mode_overshoots_where_strict_mode_does_not():
     for strict in (False, True):
         s, r = gz.compress(tx, ty, tz, eb=eb, rel_mode=True, rel_eb=float(np.float32(1e-4)), strict=strict)
         dx, dy, dz = gz.decompress(s)
-        over[strict] = gz.verify(tx, ty, tz, dx, dy, dz, eb, r.seg_size).over_bound
+        hdr = gz.parse_header(s[:32].cpu().numpy().tobytes())
+        over[strict] = gz.verify(tx, ty, tz, dx, dy, dz, hdr["eb"], r.seg_size, bound=eb).over_bound
     assert over[False] > 0 and over[True] == 0, over
