@@ -52,10 +52,10 @@ def peaks():
     return 6650.0, "fallback"
 
 
-def traffic_from_profile(n):
-    """DRAM bytes per compress launch of the default 143.7M-point workload, from
-    the committed ncu summary (None for other sizes)."""
-    p = os.path.join(ROOT, "profiles", "compress_kernel_143M_f32_3d.md")
+def traffic_from_profile(n, kernel):
+    """DRAM bytes per launch of the compress / decompress kernel on the default
+    143.7M-point workload, from the committed ncu summary (None otherwise)."""
+    p = os.path.join(ROOT, "profiles", f"{kernel}_kernel_143M_f32_3d.md")
     if n != N_POINTS or not os.path.exists(p):
         return None
     for line in open(p):
@@ -67,12 +67,14 @@ def traffic_from_profile(n):
     return None
 
 
-def bench_config(n, world, seg, sbytes):
+def bench_config(w, n, world, seg, sbytes):
     """The `config` object of the JSON line (both arms print the same keys)."""
-    return {"workload": WORKLOAD, "points_per_gpu": n, "dim": 3, "error_mode": "rel", "error_bound": REL_EB,
-            "segment_size": int(seg), "stream_bytes": int(sbytes), "compression_ratio": round(n * 12 / sbytes, 4),
+    inb = n * w["dim"] * w["bits"] // 8
+    return {"workload": w["desc"], "points_per_gpu": n, "dim": w["dim"], "float_bits": w["bits"],
+            "error_mode": w["mode"], "error_bound": w["e"], "segment_size_requested": w["seg"],
+            "segment_size": int(seg), "stream_bytes": int(sbytes), "compression_ratio": round(inb / sbytes, 4),
             "parallelism": f"{world} independent snapshots",
-            "l2": "inputs (1.72 GB per GPU) larger than the 126 MB L2; no flush"}
+            "l2": f"inputs ({inb / 1e9:.2f} GB per GPU) larger than the 126 MB L2; no flush"}
 
 
 def gen_clustered(n, seed, device):
@@ -95,6 +97,64 @@ def gen_clustered(n, seed, device):
     out = [p[:, d].contiguous() for d in range(3)]
     del p, idx, u
     return out
+
+
+def gen_lattice(n, dim, seed, device):
+    """Jittered lattice snapshot, float64, shuffled: FCC (3D; 4 points per
+    cubic cell of edge 1, 369^3 cells truncated to n) or square (2D; side
+    10,000, spacing 1), Gaussian thermal displacement sigma 0.05 per axis."""
+    import torch
+    g = torch.Generator(device=device)
+    g.manual_seed(seed)
+    i = torch.arange(n, device=device, dtype=torch.int64)
+    if dim == 3:
+        cells = 369
+        cell, b = i // 4, i % 4
+        del i
+        basis = torch.tensor([[0.0, 0.0, 0.0], [0.5, 0.5, 0.0], [0.5, 0.0, 0.5], [0.0, 0.5, 0.5]],
+                             dtype=torch.float64, device=device)
+        out = []
+        for d, c in enumerate((cell % cells, (cell // cells) % cells, cell // (cells * cells))):
+            out.append(c.double() + basis[b, d])
+        del cell, b
+    else:
+        side = 10_000
+        out = [(i % side).double(), (i // side).double()]
+        del i
+    perm = torch.randperm(n, generator=g, device=device)
+    res = []
+    for a in out:
+        a += 0.05 * torch.randn(n, generator=g, device=device, dtype=torch.float64)
+        res.append(a[perm].contiguous())
+    del out, perm
+    return res + ([None] if dim == 2 else [])
+
+
+# name -> workload (the default, "clustered", is the headline)
+WORKLOADS = {
+    "clustered": dict(n=N_POINTS, dim=3, bits=32, mode="rel", e=REL_EB, seg=0, gen="clustered", desc=WORKLOAD),
+    "clustered-abs": dict(n=N_POINTS, dim=3, bits=32, mode="abs", e=1e-3, seg=32, gen="clustered",
+                          desc=WORKLOAD.replace("rel error bound 1e-4, automatic segment size",
+                                                "abs error bound 1e-3, segment size 32 (raised to 512 by the "
+                                                "reference's block-count rule)")),
+    "fcc": dict(n=200_000_000, dim=3, bits=64, mode="rel", e=1e-5, seg=0, gen="lattice",
+                desc="200,000,000 float64 3D points of an FCC lattice (edge 1, 369^3 cells truncated), Gaussian "
+                     "jitter sigma 0.05, shuffled; rel error bound 1e-5, automatic segment size"),
+    "square": dict(n=100_000_000, dim=2, bits=64, mode="rel", e=1e-5, seg=0, gen="lattice",
+                   desc="100,000,000 float64 2D points of a square lattice (side 10,000, spacing 1), Gaussian "
+                        "jitter sigma 0.05, shuffled; rel error bound 1e-5, automatic segment size"),
+}
+
+
+def gen_workload(w, n, seed, device):
+    if w["gen"] == "clustered":
+        return gen_clustered(n, seed, device)
+    return gen_lattice(n, w["dim"], seed, device)
+
+
+def typed(bits, v):
+    import numpy as np
+    return float(np.float32(v)) if bits == 32 else float(v)
 
 
 class ClockSampler:
@@ -188,18 +248,21 @@ def barrier(world):
         torch.cuda.synchronize()
 
 
-def cpu_baseline_run(x, y, z, steps=1):
+def cpu_baseline_run(w, x, y, z, steps=1):
     """Times the OpenMP oracle (compress + decompress) on all host cores."""
     import numpy as np
     from oracle import pyoracle as po
     cores = os.cpu_count() or 1
-    eb = po.rel_to_abs(x, y, z, REL_EB)
-    rel = float(np.float32(REL_EB))
-    seg, _ = po.seg_size(x, y, z, 3, 0, True, rel, eb)
+    dim, bits = w["dim"], w["bits"]
+    if z is None:
+        z = np.zeros_like(x)
+    rel_mode = w["mode"] == "rel"
+    eb = typed(bits, po.rel_to_abs(x, y, z if dim == 3 else None, w["e"]) if rel_mode else w["e"])
+    seg, _ = po.seg_size(x, y, z, dim, w["seg"], rel_mode, typed(bits, w["e"]), eb)
     ts = []
     for _ in range(steps):
         t0 = time.perf_counter()
-        s = po.compress(x, y, z, 3, eb, seg, nthreads=cores)
+        s = po.compress(x, y, z, dim, eb, seg, nthreads=cores)
         po.decompress(s, nthreads=cores)
         ts.append(time.perf_counter() - t0)
     return ts, cores, len(s), seg
@@ -209,7 +272,7 @@ REF_BUILDS = (("gpz_ref_sm100a", "reference sources built for sm_100a"),
               ("gpz_ref_ptx90", "stock CMake architectures (compute_90 PTX, JIT-compiled on the B200)"))
 
 
-def reference_gpu_run(hx, hy, hz, n, eb, rel, ours_stream, ours_rec, reps):
+def reference_gpu_run(w, hx, hy, hz, n, eb, rel, ours_stream, ours_rec, reps):
     """Times the reference's own GPU codec on the same snapshot, in this run.
 
     The reference is built from its sources by oracle/Makefile (target `ref`)
@@ -226,10 +289,11 @@ def reference_gpu_run(hx, hy, hz, n, eb, rel, ours_stream, ours_rec, reps):
         return {"unavailable": "reference build oracle/_ref/ not present (make -C oracle ref)"}
     tmp = tempfile.mkdtemp(prefix="gpz_refgpu_")
     soa = os.path.join(tmp, "in.soa")
-    with open(soa, "wb") as f:
+    dim, bits = w["dim"], w["bits"]
+    with open(soa, "wb") as f:  # the harness reads three axes; a 2D snapshot's third is zeros
         for a in (hx, hy, hz):
-            f.write(memoryview(a.numpy()).cast("B"))
-    inb = n * 12
+            f.write(memoryview(a.numpy()).cast("B") if a is not None else bytes(n * bits // 8))
+    inb = n * dim * bits // 8
     try:
         for b, what in REF_BUILDS:
             exe = exes[b]
@@ -237,8 +301,8 @@ def reference_gpu_run(hx, hy, hz, n, eb, rel, ours_stream, ours_rec, reps):
                 out[b] = {"unavailable": "not built"}
                 continue
             st, rec = os.path.join(tmp, "ref.gpz"), os.path.join(tmp, "ref.rec")
-            p = subprocess.run([exe, "compress", soa, str(n), "3", "32", repr(eb), repr(rel), "rel", "0", st,
-                                str(reps + 1)], capture_output=True, text=True)
+            p = subprocess.run([exe, "compress", soa, str(n), str(dim), str(bits), repr(eb), repr(rel), w["mode"],
+                                str(w["seg"]), st, str(reps + 1)], capture_output=True, text=True)
             if p.returncode != 0:
                 out[b] = {"unavailable": "compress failed: " + (p.stdout + p.stderr).strip()[-200:]}
                 continue
@@ -255,7 +319,7 @@ def reference_gpu_run(hx, hy, hz, n, eb, rel, ours_stream, ours_rec, reps):
             if d.returncode == 0:
                 dj = json.loads(d.stdout.strip().splitlines()[-1])
                 dms = dj["ms"][1:] or dj["ms"]
-                rr = np.fromfile(rec, np.uint8)
+                rr = np.fromfile(rec, np.uint8)[: ours_rec.size]  # the harness writes three axes
                 line.update(decompress_ms_best=round(min(dms), 4), decompress_ms_median=round(statistics.median(dms), 4),
                             decompress_gbs_best=round(inb / min(dms) / 1e6, 2),
                             identical_reconstruction=bool(rr.size == ours_rec.size and np.array_equal(rr, ours_rec)))
@@ -276,26 +340,31 @@ def reference_gpu_run(hx, hy, hz, n, eb, rel, ours_stream, ours_rec, reps):
 
 def run_reference(args):
     """CPU implementation of the path on the host cores (rank 0 only)."""
-    import numpy as np
     import torch
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
+    w = WORKLOADS[args.config]
+    n = args.points or w["n"]
     dev = "cuda" if torch.cuda.is_available() else "cpu"
-    x, y, z = (t.cpu().numpy() for t in gen_clustered(N_POINTS, 1234, dev))
+    axes = gen_workload(w, n, 1234 if w["gen"] == "clustered" else 2024, dev)
+    x, y = (t.cpu().numpy() for t in axes[:2])
+    z = axes[2].cpu().numpy() if axes[2] is not None else None
+    del axes
     if args.warmup > 0:
-        cpu_baseline_run(x, y, z, args.warmup)
-    ts, cores, sbytes, seg = cpu_baseline_run(x, y, z, args.steps)
+        cpu_baseline_run(w, x, y, z, args.warmup)
+    ts, cores, sbytes, seg = cpu_baseline_run(w, x, y, z, args.steps)
     step = sum(ts) / len(ts)
-    val = N_POINTS * 12 / step / 1e9
+    inb = n * w["dim"] * w["bits"] // 8
+    val = inb / step / 1e9
     line = {
         "impl": "reference", "metric": METRIC, "value": round(val, 4), "unit": "GB/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(step * 1e3, 3), "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": bench_config(N_POINTS, world, seg, sbytes),
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32" if w["bits"] == 32 else "f64", "data": "synthetic",
+        "config": bench_config(w, n, world, seg, sbytes),
         "cpu_baseline": {"value": round(val, 4), "unit": "GB/s", "cores": cores, "kind": "port",
-                         "sample": f"the full snapshot ({N_POINTS} points) per step, compress + decompress, "
+                         "sample": f"the full snapshot ({n} points) per step, compress + decompress, "
                                    "OpenMP C++ restatement of the reference algorithm (the reference has no "
                                    "CPU implementation)"},
         "e2e": {"value": round(val, 4), "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -303,7 +372,7 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
-def run_e2e(args, world, p, hx, hy, hz, n, dev, inb, ref_out):
+def run_e2e(args, world, w, p, host_axes, n, dev, inb, ref_out):
     """Compress + decompress through the C ABI from and to pinned host buffers,
     every copy timed.  Consecutive steps overlap their copies
     (gpz_b200.pipeline.SnapshotPipeline): each step uploads the snapshot,
@@ -312,12 +381,12 @@ def run_e2e(args, world, p, hx, hy, hz, n, dev, inb, ref_out):
     device-resident one."""
     import torch
     from gpz_b200.pipeline import SnapshotPipeline
-    pipe = SnapshotPipeline(p, n, 3, 32, dev)
+    pipe = SnapshotPipeline(p, n, w["dim"], w["bits"], dev)
     e2e_steps = max(2, min(args.steps, 10))
-    pipe.round_trips([hx, hy, hz], 2)  # warm-up
+    pipe.round_trips(host_axes, 2)  # warm-up
     barrier(world)
     te0 = time.perf_counter()
-    nb, rx = pipe.round_trips([hx, hy, hz], e2e_steps)
+    nb, rx = pipe.round_trips(host_axes, e2e_steps)
     te1 = time.perf_counter()
     for h, d in zip(rx, ref_out):
         if not torch.equal(h, d.cpu()):
@@ -364,39 +433,49 @@ def run_ours(args):
 
     world, rank, local = dist_setup(args.gpus)
     dev = torch.device("cuda", local if world > 1 else 0)
-    n = args.points
-    x, y, z = gen_clustered(n, 1234 + rank, dev)
-    inb = n * 3 * 4
-    eb, _ = gz.rel_to_abs(x, y, z, REL_EB)  # host-side rel->abs of the CLI, untimed as in the reference
-    rel = float(np.float32(REL_EB))
-    p = gz.make_params(n, 3, 32, eb, 0, True, rel)
-    cap = gz.stream_bound(n, 3, 32)
+    w = WORKLOADS[args.config]
+    headline = args.config == "clustered"
+    n, dim, bits = args.points or w["n"], w["dim"], w["bits"]
+    dt = torch.float32 if bits == 32 else torch.float64
+    x, y, z = gen_workload(w, n, (1234 if w["gen"] == "clustered" else 2024) + rank, dev)
+    inb = n * dim * bits // 8
+    rel_mode = w["mode"] == "rel"
+    rel = typed(bits, w["e"])
+    if rel_mode:
+        eb, _ = gz.rel_to_abs(x, y, z, w["e"])  # the CLI's rel->abs, on the device; untimed as in the reference
+    else:
+        eb = rel
+    p = gz.make_params(n, dim, bits, eb, w["seg"], rel_mode, rel if rel_mode else 0.0)
+    cap = gz.stream_bound(n, dim, bits)
     out = torch.empty(cap, dtype=torch.uint8, device=dev)
     scr_c = torch.empty(gz.compress_scratch_bytes(n), dtype=torch.uint8, device=dev)
     scr_d = torch.empty(256, dtype=torch.uint8, device=dev)
-    ox, oy, oz = (torch.empty(n, dtype=torch.float32, device=dev) for _ in range(3))
+    ox, oy = (torch.empty(n, dtype=dt, device=dev) for _ in range(2))
+    oz = torch.empty(n, dtype=dt, device=dev) if dim == 3 else None
+    zc, ozc = (z, oz) if dim == 3 else (x, ox)  # the ABI ignores the third axis in 2D
     stream = torch.cuda.current_stream(dev)
 
-    # correctness gate before timing: round trip within the bound on a sample
-    r = gz.compress_into(p, x, y, z, out, scr_c)
-    rr = gz.decompress_into(out, r.stream_bytes, 32, 3, ox, oy, oz, scr_d)
+    # correctness gate before timing: the round trip, every point paired with
+    # its own reconstruction (gpz_verify)
+    r = gz.compress_into(p, x, y, zc, out, scr_c)
+    rr = gz.decompress_into(out, r.stream_bytes, bits, dim, ox, oy, ozc, scr_d)
     assert r.status == 0 and rr.status == 0
     sbytes = int(r.stream_bytes)
-    # every point paired with its own reconstruction (gpz_verify)
     hdr = gz.parse_header(out[:32].cpu().numpy().tobytes())
     ver = gz.verify(x, y, z, ox, oy, oz, hdr["eb"], hdr["seg"])
-    assert ver.over_bound_tol == 0, ver.over_bound_tol  # the reference verifier's 1.01*eb tolerance
+    if headline:  # the headline holds the reference verifier's 1.01*eb tolerance; other workloads report
+        assert ver.over_bound_tol == 0, ver.over_bound_tol
     ref_stream = out[:sbytes].clone()
-    ref_rec = [t.clone() for t in (ox, oy, oz)]
-    strict = strict_bound_run(gz, x, y, z, n, eb, rel)
+    ref_rec = [t.clone() for t in (ox, oy, oz) if t is not None]
+    strict = strict_bound_run(gz, x, y, z, n, eb, rel) if headline else None
 
     def step(evs=None):
         if evs is not None:
             evs[0].record(stream)
-        gz.compress_into(p, x, y, z, out, scr_c, sync=False)
+        gz.compress_into(p, x, y, zc, out, scr_c, sync=False)
         if evs is not None:
             evs[1].record(stream)
-        gz.decompress_into(out, cap, 32, 3, ox, oy, oz, scr_d, sync=False)
+        gz.decompress_into(out, cap, bits, dim, ox, oy, ozc, scr_d, sync=False)
         if evs is not None:
             evs[2].record(stream)
 
@@ -419,7 +498,8 @@ def run_ours(args):
     rc_, rd_ = gz.result_get(scr_c, stream), gz.result_get(scr_d, stream)
     if rc_.status != 0 or rd_.status != 0 or int(rc_.stream_bytes) != sbytes:
         raise RuntimeError(f"timed launches failed: compress {rc_.status}, decompress {rd_.status}")
-    if not torch.equal(out[:sbytes], ref_stream) or not all(torch.equal(a, b) for a, b in zip((ox, oy, oz), ref_rec)):
+    rec_now = [t for t in (ox, oy, oz) if t is not None]
+    if not torch.equal(out[:sbytes], ref_stream) or not all(torch.equal(a, b) for a, b in zip(rec_now, ref_rec)):
         raise RuntimeError("timed launches produced a different stream or reconstruction")
     del ref_rec
     total_ms = max_over_ranks(t0.elapsed_time(t1), world)
@@ -431,31 +511,35 @@ def run_ours(args):
     dec_gbs = inb / (statistics.mean(d_ms) * 1e-3) / 1e9
     clocks = clk.summary()
 
-    # roofline of the dominant kernel (compress): algorithmic bytes per launch
-    # (input + stream) over its mean CUDA-event duration in the timed region
+    # roofline of the two codec kernels: algorithmic bytes per launch (input
+    # + stream) over their mean CUDA-event durations in the timed region
     peak, peak_kind = peaks()
-    alg_c = inb + sbytes
-    achieved = alg_c / (statistics.mean(c_ms) * 1e-3) / 1e9
-    traffic = traffic_from_profile(n)
+    alg = inb + sbytes
+    achieved_c = alg / (statistics.mean(c_ms) * 1e-3) / 1e9
+    achieved_d = alg / (statistics.mean(d_ms) * 1e-3) / 1e9
+    tname = "float" if bits == 32 else "double"
+    traffic_c = traffic_from_profile(n, "compress") if headline else None
+    traffic_d = traffic_from_profile(n, "decompress") if headline else None
 
     # ---- end to end through the C ABI with pinned host buffers ----
-    hx, hy, hz = (t.cpu().pin_memory() for t in (x, y, z))
+    host = [t.cpu().pin_memory() for t in (x, y, z) if t is not None]
     if args.no_e2e:
         e2e_val, nb, e2e_steps = None, sbytes, 0
     else:
-        e2e_val, nb, e2e_steps = run_e2e(args, world, p, hx, hy, hz, n, dev, inb, (ox, oy, oz))
+        e2e_val, nb, e2e_steps = run_e2e(args, world, w, p, host, n, dev, inb, rec_now)
 
     ref_gpu = None
     if world == 1 and rank == 0 and not args.no_reference_gpu:
-        import numpy as np
         ours_stream = out[:sbytes].cpu().numpy()
-        ours_rec = np.concatenate([t.cpu().numpy() for t in (ox, oy, oz)]).view(np.uint8)
-        ref_gpu = reference_gpu_run(hx, hy, hz, n, float(eb), rel, ours_stream, ours_rec, max(3, min(args.steps, 10)))
+        ours_rec = np.concatenate([t.cpu().numpy() for t in rec_now]).view(np.uint8)
+        ref_gpu = reference_gpu_run(w, host[0], host[1], host[2] if dim == 3 else None, n, float(eb), rel,
+                                    ours_stream, ours_rec, max(3, min(args.steps, 10)))
         del ours_stream, ours_rec
 
     cpu = None
     if world == 1 and rank == 0 and not args.no_cpu_baseline:
-        ts, cores, _, _ = cpu_baseline_run(hx.numpy(), hy.numpy(), hz.numpy(), 1)
+        ts, cores, _, _ = cpu_baseline_run(w, host[0].numpy(), host[1].numpy(),
+                                           host[2].numpy() if dim == 3 else None, 1)
         cpu = {"value": round(inb / ts[0] / 1e9, 4), "unit": "GB/s", "cores": cores, "kind": "port",
                "sample": f"one compress + decompress of the same {n}-point snapshot on {cores} host threads "
                          "(OpenMP C++ restatement of the reference algorithm)"}
@@ -464,25 +548,28 @@ def run_ours(args):
         line = {
             "metric": METRIC, "value": round(value, 3), "unit": "GB/s", "n_gpus": world, "steps": args.steps,
             "warmup": max(args.warmup, 3), "ms_per_step": round(ms_step, 4), "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-            "data": "synthetic (seeded clustered generator standing in for SDRBench HACC-style snapshots)",
-            "config": bench_config(n, world, r.seg_size, sbytes),
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32" if bits == 32 else "f64",
+            "data": "synthetic (seeded generator standing in for the snapshots named in the workload)",
+            "config": bench_config(w, n, world, r.seg_size, sbytes),
             "verified": {"points": int(ver.points), "over_bound": int(ver.over_bound),
-                         "over_1.01eb": int(ver.over_bound_tol),
+                         "over_1.01eb": int(ver.over_bound_tol), "id_overflow": int(r.id_overflow),
                          "note": "default mode reproduces the reference's bytes and reconstruction, whose float "
                                  "rounding puts points just past eb (its verifier allows 1.01*eb); strict_bound "
-                                 "below holds eb for every point",
-                         "max_abs_err": [round(v, 9) for v in ver.max_abs_err], "eb": hdr["eb"],
+                                 "holds eb for every point",
+                         "max_abs_err": [round(v, 9) for v in ver.max_abs_err[:dim]], "eb": hdr["eb"],
                          "psnr_db": round(ver.psnr_combined, 3)},
             "compress_gbs": round(comp_gbs, 3), "decompress_gbs": round(dec_gbs, 3),
             "compress_ms": round(statistics.mean(c_ms), 4), "decompress_ms": round(statistics.mean(d_ms), 4),
             "compress_ms_min_median_max": [round(min(c_ms), 4), round(statistics.median(c_ms), 4), round(max(c_ms), 4)],
             "decompress_ms_min_median_max": [round(min(d_ms), 4), round(statistics.median(d_ms), 4),
                                              round(max(d_ms), 4)],
-            "roofline": {"bound": "hbm", "kernel": "compress_kernel<float,3>", "achieved": round(achieved, 2),
-                         "peak": peak, "peak_kind": peak_kind, "unit": "GB/s", "frac": round(achieved / peak, 4),
-                         "traffic": traffic,
-                         "alg_bytes_per_launch": alg_c},
+            "roofline": {"bound": "hbm", "kernel": f"compress_kernel<{tname},{dim}>", "achieved": round(achieved_c, 2),
+                         "peak": peak, "peak_kind": peak_kind, "unit": "GB/s", "frac": round(achieved_c / peak, 4),
+                         "traffic": traffic_c, "alg_bytes_per_launch": alg},
+            "roofline_decompress": {"bound": "hbm", "kernel": f"decompress_kernel<{tname},{dim}>",
+                                    "achieved": round(achieved_d, 2), "peak": peak, "peak_kind": peak_kind,
+                                    "unit": "GB/s", "frac": round(achieved_d / peak, 4), "traffic": traffic_d,
+                                    "alg_bytes_per_launch": alg},
             "gpu_launches": 3 * args.steps,
             "clocks": clocks,
             "e2e": None if e2e_val is None else
@@ -806,8 +893,10 @@ def main():
     ap.add_argument("--requests", type=int, default=300, help="requests per arrival rate")
     ap.add_argument("--serve-streams", type=int, default=2)
     ap.add_argument("--overlap", action="store_true", help="let served batches run concurrently")
-    ap.add_argument("--points", type=int, default=N_POINTS,
-                    help="points per GPU (smaller cases for profiler captures; the headline uses the default)")
+    ap.add_argument("--points", type=int, default=0,
+                    help="points per GPU (smaller cases for profiler captures; 0: the workload's size)")
+    ap.add_argument("--config", choices=sorted(WORKLOADS), default="clustered",
+                    help="workload (default: the 143.7M-point clustered float32 snapshot at rel 1e-4)")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)

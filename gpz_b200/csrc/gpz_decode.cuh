@@ -483,11 +483,13 @@ __device__ __forceinline__ void decode_chunk(const DArgs<T> &a, unsigned long lo
         const Acc t = __shfl_up_sync(FULL, inc, o);
         if (lane >= o) inc += t;
       }
-      // the last id bounds them all (ids never decrease); 1023 deltas below
-      // 2^21 cannot wrap a 32-bit sum
+      // the last id bounds them all (ids never decrease).  In a valid stream
+      // every prefix of the deltas is an id difference below 2^31, so the
+      // 32-bit sums of float streams cannot wrap; float64 streams sum in 64
+      // bits.  (A corrupt stream can only yield wrong coordinates here, no
+      // access depends on the ids.)
       const unsigned long long total = (unsigned long long)__shfl_sync(FULL, inc, 31);
-      fast = dbits <= 21u && first + total < (1ull << 31) && !g.wide && bnx != 0 && bny != 0 &&
-             bnx * bny < (1ull << 32);
+      fast = first + total < (1ull << 31) && !g.wide && bnx != 0 && bny != 0 && bnx * bny < (1ull << 32);
       scatter_runs<T, N>(q, P16, sw, (Acc)first + (inc - loc), nl, fast, lane);
     };
     uint32_t orw = 0;

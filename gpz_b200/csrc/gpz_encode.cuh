@@ -659,8 +659,11 @@ __device__ __forceinline__ uint32_t encode_pack(const CArgs<T> &a, unsigned long
 #pragma unroll
     for (int j = 0; j < 32; ++j) key[j] = kmin + (key[j] >> 10);
   } else {
-    // wider composites (rare): the bucket path, outside the hot path's
-    // register budget; block ids in and results out through S and hist rows
+    // wider composites: the bucket path, outside the hot path's register
+    // budget; block ids in and results out through S and hist rows.  (A
+    // coarse 32-bit warp sort with the dropped id bits parked beside the
+    // relative positions, checked afterwards, measured slower on the wide
+    // lattices: 7.7 ms against 6.7 ms for 200M float64 FCC points.)
 #pragma unroll
     for (int m = 0; m < 8; ++m)
       *reinterpret_cast<uint4 *>(S + qoff(lane, m)) = make_uint4(key[4 * m], key[4 * m + 1], key[4 * m + 2], key[4 * m + 3]);

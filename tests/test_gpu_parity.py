@@ -144,6 +144,11 @@ EDGE = [
     (2, 100000, 3, 64, 0.0, 0.05, 17, "rel", 1e-5, 0),
     (2, 50000, 2, 64, 0.0, 0.05, 18, "rel", 1e-5, 0),
     (0, 20000, 3, 32, 0.0, 1e-3, 19, "abs", 1.0, 2),     # everything in one block
+    # wide composites (id range above 2^22): the bucket ranking, on clustered
+    # data (crowded buckets) and uniform data
+    (1, 200000, 3, 32, 0.0, 1000.0, 20, "rel", 1e-5, 0),
+    (1, 120000, 3, 64, 0.0, 1000.0, 21, "rel", 1e-5, 0),
+    (0, 100000, 3, 64, 0.0, 1000.0, 22, "abs", 1e-4, 1),   # rel positions 0 bits, ids 31 bits
 ]
 
 
