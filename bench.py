@@ -467,7 +467,7 @@ def run_ours(args):
         assert ver.over_bound_tol == 0, ver.over_bound_tol
     ref_stream = out[:sbytes].clone()
     ref_rec = [t.clone() for t in (ox, oy, oz) if t is not None]
-    strict = strict_bound_run(gz, x, y, z, n, eb, rel) if headline else None
+    strict = strict_bound_run(gz, x, y, z, n, eb, rel) if headline and not args.no_strict else None
 
     def step(evs=None):
         if evs is not None:
@@ -697,6 +697,51 @@ def run_batched(args):
 
     t_pd = ev_time(plain_decompress, args.steps)
     torch.cuda.synchronize()
+
+    # ---- where the ceiling is: per-snapshot plain times (each call between
+    # its own events, calls back to back) split at one wave of the persistent
+    # compress grid.  A snapshot of a wave or more keeps every SM busy on its
+    # own, so batching can at best run the smaller ones at the rate the large
+    # ones reach: ceiling = plain / (plain of the large + small bytes / that
+    # rate).
+    def per_call_ms(calls):
+        for fn in calls:
+            fn()
+        torch.cuda.synchronize()
+        evs_ = [torch.cuda.Event(enable_timing=True) for _ in range(len(calls) + 1)]
+        evs_[0].record(stream)
+        for fn, e in zip(calls, evs_[1:]):
+            fn()
+            e.record(stream)
+        torch.cuda.synchronize()
+        return [a.elapsed_time(b) for a, b in zip(evs_[:-1], evs_[1:])]
+
+    nb_snap = [x.numel() * (3 if z is not None else 2) * (4 if x.dtype == torch.float32 else 8)
+               for x, _, z, _ in snaps]
+    wave_chunks = 2 * 148 * 8  # resident CTAs x SMs x chunks per CTA on a B200
+    large = [x.numel() >= wave_chunks * 1024 for x, _, _, _ in snaps]
+    c_calls = [(lambda x=x, y=y, z=z, p=p, o=o, sc=sc: gz.compress_into(p, x, y, z if z is not None else x, o, sc,
+                                                                         stream, sync=False))
+               for (x, y, z, _), p, o, sc in zip(snaps, params, plain_out, plain_scr)]
+    d_calls = [(lambda s_b=s_b, ox=ox, oy=oy, oz=oz, x=x, z=z, sc=sc: gz.decompress_into(
+                    s_b, s_b.numel(), 32 if x.dtype == torch.float32 else 64, 3 if z is not None else 2, ox, oy,
+                    oz if z is not None else ox, sc, stream, sync=False))
+               for s_b, (ox, oy, oz), (x, _, z, _), sc in zip(streams, dec_out, snaps, dscr)]
+
+    def ceiling(ms):
+        lb = sum(b for b, l in zip(nb_snap, large) if l)
+        lm = sum(t for t, l in zip(ms, large) if l)
+        sb = sum(b for b, l in zip(nb_snap, large) if not l)
+        sm = sum(t for t, l in zip(ms, large) if not l)
+        rate = lb / lm if lm > 0 else float("nan")  # bytes per ms
+        best = lm + sb / rate
+        return {"large_snapshots": sum(large), "large_bytes": lb, "large_plain_ms": round(lm, 3),
+                "small_snapshots": len(large) - sum(large), "small_bytes": sb, "small_plain_ms": round(sm, 3),
+                "large_rate_gbs": round(rate / 1e6, 2), "best_case_ms": round(best, 3),
+                "ceiling_speedup": round((lm + sm) / best, 3)}
+
+    ceil_c = ceiling(per_call_ms(c_calls))
+    ceil_d = ceiling(per_call_ms(d_calls))
     for (ox, oy, oz), (bx, by, bz) in zip(dec_out, d.outputs):
         for a, c in ((ox, bx), (oy, by), (oz, bz)):
             if a is not None:
@@ -753,6 +798,10 @@ def run_batched(args):
                       "segments_changed": sum(a != b for a, b in zip(segs_default, segs_tuned)),
                       "candidates": [1, 2, 4, 8, 16, 32, 64, 128], "sample_points": 1 << 17},
         "identical_output": bool(same),
+        "ceiling": {"note": "snapshots of at least one wave of the persistent compress grid (2 CTAs x 148 SMs x 8 "
+                            "chunks = 2,424,832 points) keep the GPU busy alone; the best a batch can do is run "
+                            "the smaller ones at the large ones' rate",
+                    "wave_points": wave_chunks * 1024, "compress": ceil_c, "decompress": ceil_d},
     }
     b.close()
     d.close()
@@ -884,6 +933,7 @@ def main():
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer end-to-end timing")
     ap.add_argument("--no-reference-gpu", action="store_true",
                     help="skip timing the reference's own GPU build on the same snapshot")
+    ap.add_argument("--no-strict", action="store_true", help="skip the strict-bound runs")
     ap.add_argument("--batched", action="store_true",
                     help="time the batched form (many snapshots per graph launch) against per-snapshot calls")
     ap.add_argument("--batch", type=int, default=256, help="snapshots in the batched workload")

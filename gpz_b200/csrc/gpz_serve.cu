@@ -275,8 +275,19 @@ struct gpz_server {
         return false;
       }
     }
-    // without GPZ_SERVER_OVERLAP the GPU runs batches in launch order
+    // without GPZ_SERVER_OVERLAP the GPU runs batches in launch order; with
+    // it, batches on different slots run at once, each persistent grid sized
+    // to its slot's share of the SMs, so concurrent batches split the GPU
+    // instead of competing for residency with full-occupancy grids
     if (!(cfg.flags & GPZ_SERVER_OVERLAP) && last) cudaStreamWaitEvent(s.st, last, 0);
+    if ((cfg.flags & GPZ_SERVER_OVERLAP) && cfg.streams > 1) {
+      for (int c = 0; c < 4; ++c) {
+        if (!ci.empty() && Lc.cls[c].grid > 0)
+          Lc.cls[c].grid = std::max(1, (int)((Lc.cls[c].grid + cfg.streams - 1) / cfg.streams));
+        if (!di.empty() && Ld.cls[c].grid > 0)
+          Ld.cls[c].grid = std::max(1, (int)((Ld.cls[c].grid + cfg.streams - 1) / cfg.streams));
+      }
+    }
     uint8_t *ws = arena.base + s.ws_off;
     uint8_t *wsd = ws + (ci.empty() ? 0 : up(Lc.bytes));
     uint8_t *img = s.image;
