@@ -126,18 +126,30 @@ int decompress_t(const void *d_stream, uint64_t stream_bytes, uint32_t dim, void
   a.vec_ok = aligned16(d_x) && aligned16(d_y) && (dim == 2 || aligned16(d_z));
   // The chunk count lives in the device header: one warp per chunk in a grid
   // of at most one full wave, each warp striding over the chunks.
-  constexpr int W = DecCfg<T>::warps;
-  constexpr size_t smem = dec_smem_bytes<T>();
-  const uint64_t bound_ctas = (stream_bytes / (8ull + TT<T>::meta) + W) / W;
   NvtxRange krange("run decompress kernel");
-  auto launch = [&](auto kernel) -> bool {
+  auto launch = [&](auto kernel, auto cfg) -> bool {
+    using Cfg = decltype(cfg);
+    constexpr int W = Cfg::warps;
+    constexpr size_t smem = dec_smem_bytes_of<Cfg>();
+    const uint64_t bound_ctas = (stream_bytes / (8ull + TT<T>::meta) + W) / W;
     const int occ = resident_ctas(kernel, 32 * W, smem);
     if (occ == 0) return false;
     const uint64_t grid = std::min<uint64_t>((uint64_t)num_sms() * occ, bound_ctas);
     kernel<<<(unsigned)grid, 32 * W, smem, st>>>(a);
     return true;
   };
-  if (!(dim == 3 ? launch(decompress_kernel<T, 3>) : launch(decompress_kernel<T, 2>))) return GPZ_ECUDA;
+  if constexpr (sizeof(T) == 4) {
+    if (!(dim == 3 ? launch(decompress_kernel<T, 3>, DecCfg<T>{}) : launch(decompress_kernel<T, 2>, DecCfg<T>{})))
+      return GPZ_ECUDA;
+  } else {
+    // fast pass in the 12 KB layout, then the general pass for the chunks it
+    // left (it returns at once when there are none)
+    bool ok = dim == 3 ? launch(decompress_kernel<T, 3, DecCfgF64Fast, kPassFast>, DecCfgF64Fast{})
+                       : launch(decompress_kernel<T, 2, DecCfgF64Fast, kPassFast>, DecCfgF64Fast{});
+    ok = ok && (dim == 3 ? launch(decompress_kernel<T, 3, DecCfg<T>, kPassGeneral>, DecCfg<T>{})
+                         : launch(decompress_kernel<T, 2, DecCfg<T>, kPassGeneral>, DecCfg<T>{}));
+    if (!ok) return GPZ_ECUDA;
+  }
   return cuda_status(cudaGetLastError());
 }
 

@@ -54,6 +54,23 @@ template <> struct DecCfg<double> {
 template <typename T>
 constexpr size_t dec_smem_bytes() { return (size_t)DecCfg<T>::warps * DecCfg<T>::words * 4; }
 
+// Float64 streams whose chunks have ordinary geometry (block counts whose
+// product fits 32 bits; ids are below 2^31 in every valid stream) need no
+// 64-bit id tables: they decode in the float layout, 12 KB per warp, twice
+// the warps per SM of the general layout.  A chunk with wider geometry is
+// left to a second pass in the general layout.
+struct DecCfgF64Fast {
+  static constexpr int warps = 4, min_ctas = 4;
+  static constexpr int A = 0, P = 0, TL = kChunk, TH = kChunk, R = kChunk, C = 2 * kChunk, words = 3 * kChunk;
+};
+template <class Cfg>
+constexpr size_t dec_smem_bytes_of() { return (size_t)Cfg::warps * Cfg::words * 4; }
+
+// Which chunks a decompress pass decodes.
+constexpr int kPassAll = 0;      // every chunk (general layout)
+constexpr int kPassFast = 1;     // chunks of ordinary geometry; the others are flagged in ctl->deferred
+constexpr int kPassGeneral = 2;  // only the chunks kPassFast left (general layout)
+
 // ---------------------------------------------------------------------------
 // Bit planes.  Delta and count planes are ceil(U/8) bytes each, MSB plane
 // first, element k at bit 7-(k%8) of byte k/8 (src/cudaWarpCompress.cu:366-378);
@@ -202,10 +219,9 @@ __device__ __forceinline__ void copy_out_rows(const uint32_t *stage, T *dst, int
 // id/(bnx*bny) (axis 2), each axis leaving the next quotient in place.
 // MODE 1: P holds 32-bit ids, general dividers.  MODE 2 (double streams): P
 // holds run indices, 64-bit ids come from the id table.
-template <typename T, int D, int MODE, bool KEEP>
+template <typename T, int D, int MODE, bool KEEP, class Cfg>
 __device__ __forceinline__ void reconstruct_axis(uint32_t *sw, const ChunkGeom &g, T eb, T mn, T *dst, int lane,
                                                  uint32_t nvalid, bool full) {
-  using Cfg = DecCfg<T>;
   constexpr bool is64 = sizeof(T) == 8;
   constexpr int H = is64 ? 2 : 1;  // staged (half-)rows per axis
   uint32_t *P = sw + Cfg::P;
@@ -265,12 +281,12 @@ __device__ __forceinline__ void reconstruct_axis(uint32_t *sw, const ChunkGeom &
   }
 }
 
-template <typename T, int DIM, int MODE>
+template <typename T, int DIM, int MODE, class Cfg>
 __device__ __forceinline__ void reconstruct(uint32_t *sw, const ChunkGeom &g, T eb, const T (&mm)[6], T *const (&Y)[3],
                                             unsigned long long base, int lane, uint32_t nvalid, bool full) {
-  reconstruct_axis<T, 0, MODE, true>(sw, g, eb, mm[0], Y[0] + base, lane, nvalid, full);
-  reconstruct_axis<T, 1, MODE, DIM == 3>(sw, g, eb, mm[1], Y[1] + base, lane, nvalid, full);
-  if constexpr (DIM == 3) reconstruct_axis<T, 2, MODE, false>(sw, g, eb, mm[2], Y[2] + base, lane, nvalid, full);
+  reconstruct_axis<T, 0, MODE, true, Cfg>(sw, g, eb, mm[0], Y[0] + base, lane, nvalid, full);
+  reconstruct_axis<T, 1, MODE, DIM == 3, Cfg>(sw, g, eb, mm[1], Y[1] + base, lane, nvalid, full);
+  if constexpr (DIM == 3) reconstruct_axis<T, 2, MODE, false, Cfg>(sw, g, eb, mm[2], Y[2] + base, lane, nvalid, full);
 }
 
 template <typename T>
@@ -285,10 +301,9 @@ __device__ __forceinline__ uint32_t dec_meta_word(const uint8_t *s, unsigned lon
 
 // Deltas -> run ids -> run map (and id table on the general path).  Called
 // with the section words of width N; P16 holds the run starts as 16-bit pairs.
-template <typename T, int N>
+template <typename T, int N, class Cfg>
 __device__ __forceinline__ void scatter_runs(const uint32_t (&q)[N], const uint32_t (&P16)[16], uint32_t *sw,
                                              typename TT<T>::U id, uint32_t nl, bool fast, int lane) {
-  using Cfg = DecCfg<T>;
   uint32_t *A = sw + Cfg::A, *TL = sw + Cfg::TL, *TH = sw + Cfg::TH;
   if (fast) {
 #pragma unroll
@@ -318,12 +333,11 @@ __device__ __forceinline__ void scatter_runs(const uint32_t (&q)[N], const uint3
 // One chunk of a stream: c its index, n/G/pay_base/eb/seg from the validated
 // header, mwc the lanes' words of its meta record (dec_meta_word).  A record
 // or payload that fails validation sets GPZ_ESTREAM and writes nothing.
-template <typename T, int DIM>
+template <typename T, int DIM, class Cfg = DecCfg<T>, int PASS = kPassAll>
 __device__ __forceinline__ void decode_chunk(const DArgs<T> &a, unsigned long long c, unsigned long long n,
                                              unsigned long long G, unsigned long long pay_base, T eb, uint32_t seg,
                                              ChunkGeom &g, uint32_t mwc, uint32_t *sw, int lane) {
   using Tr = TT<T>;
-  using Cfg = DecCfg<T>;
   using Acc = typename TT<T>::U;
   constexpr bool is64 = sizeof(T) == 8;
   constexpr uint32_t FULL = 0xFFFFFFFFu;
@@ -390,6 +404,17 @@ __device__ __forceinline__ void decode_chunk(const DArgs<T> &a, unsigned long lo
   g.bnx64 = bnx;
   g.bny64 = bny;
   g.wide = is64 && ((bnx >> 32) != 0 || (bny >> 32) != 0 || ((bnx * bny) >> 32) != 0);
+  if constexpr (PASS != kPassAll) {
+    const bool general_geom = g.wide || bnx == 0 || bny == 0 || bnx * bny >= (1ull << 32);
+    if constexpr (PASS == kPassFast) {
+      if (general_geom) {  // left to the general pass
+        if (lane == 0) atomicExch(&ctl->deferred, 1u);
+        return;
+      }
+    } else {
+      if (!general_geom) return;  // decoded by the fast pass
+    }
+  }
   const uint32_t my_div = lane == 0 ? (uint32_t)bnx : (lane == 1 ? (uint32_t)bny : (uint32_t)(bnx * bny));
   {
     FastDiv31 d31;
@@ -458,7 +483,7 @@ __device__ __forceinline__ void decode_chunk(const DArgs<T> &a, unsigned long lo
   __syncwarp();  // run map rows cleared
 
   // ---- deltas -> ids: id[0] = first, id[u] = id[u-1] + delta[u] (:930-938) ----
-  bool fast = false;
+  bool fast = false, bail = false;
   {
     auto run_ids = [&](auto &q) {
       constexpr int N = sizeof(q) / sizeof(uint32_t);
@@ -490,7 +515,15 @@ __device__ __forceinline__ void decode_chunk(const DArgs<T> &a, unsigned long lo
       // access depends on the ids.)
       const unsigned long long total = (unsigned long long)__shfl_sync(FULL, inc, 31);
       fast = first + total < (1ull << 31) && !g.wide && bnx != 0 && bny != 0 && bnx * bny < (1ull << 32);
-      scatter_runs<T, N>(q, P16, sw, (Acc)first + (inc - loc), nl, fast, lane);
+      if constexpr (PASS == kPassFast) {
+        // the fast layout has no id tables: ids of 2^31 or more (which no
+        // valid stream holds, ids are masked to 31 bits) are rejected
+        if (!fast) {
+          bail = true;
+          return;
+        }
+      }
+      scatter_runs<T, N, Cfg>(q, P16, sw, (Acc)first + (inc - loc), nl, fast, lane);
     };
     uint32_t orw = 0;
     if (dbits <= 8u) {
@@ -506,6 +539,10 @@ __device__ __forceinline__ void decode_chunk(const DArgs<T> &a, unsigned long lo
       section_words<32>(q, rawd, pw, 0u, dbits, bpp, endd, vmd, lane, orw);
       run_ids(q);
     }
+  }
+  if (bail) {
+    if (lane == 0) set_status(ctl, kESTREAM);
+    return;
   }
   __syncwarp();
 
@@ -575,27 +612,32 @@ __device__ __forceinline__ void decode_chunk(const DArgs<T> &a, unsigned long lo
   // ---- reconstruct ----
   const bool full = nvalid == (uint32_t)kChunk && a.vec_ok;
   if (fast) {
-    reconstruct<T, DIM, 0>(sw, g, eb, mm, Y, base, lane, nvalid, full);
+    reconstruct<T, DIM, 0, Cfg>(sw, g, eb, mm, Y, base, lane, nvalid, full);
   } else {
     FastDiv f;
     f.init(my_div);
     g.fx.d = __shfl_sync(FULL, f.d, 0); g.fx.m = __shfl_sync(FULL, f.m, 0); g.fx.s = __shfl_sync(FULL, f.s, 0);
     g.fy.d = __shfl_sync(FULL, f.d, 1); g.fy.m = __shfl_sync(FULL, f.m, 1); g.fy.s = __shfl_sync(FULL, f.s, 1);
     g.fxy.d = __shfl_sync(FULL, f.d, 2); g.fxy.m = __shfl_sync(FULL, f.m, 2); g.fxy.s = __shfl_sync(FULL, f.s, 2);
-    if constexpr (!is64) reconstruct<T, DIM, 1>(sw, g, eb, mm, Y, base, lane, nvalid, full);
-    else reconstruct<T, DIM, 2>(sw, g, eb, mm, Y, base, lane, nvalid, full);
+    if constexpr (PASS != kPassFast) {
+      if constexpr (!is64) reconstruct<T, DIM, 1, Cfg>(sw, g, eb, mm, Y, base, lane, nvalid, full);
+      else reconstruct<T, DIM, 2, Cfg>(sw, g, eb, mm, Y, base, lane, nvalid, full);
+    }
   }
 }
 
-template <typename T, int DIM>
-__global__ void __launch_bounds__(32 * DecCfg<T>::warps, DecCfg<T>::min_ctas) decompress_kernel(const DArgs<T> a) {
+// Persistent decompress kernel.  Float streams: one pass (PASS kPassAll) in
+// the float layout.  Float64 streams: the fast pass in the 12 KB layout, then
+// the general pass, which returns at once unless the fast pass left chunks.
+template <typename T, int DIM, class Cfg = DecCfg<T>, int PASS = kPassAll>
+__global__ void __launch_bounds__(32 * Cfg::warps, Cfg::min_ctas) decompress_kernel(const DArgs<T> a) {
   using Tr = TT<T>;
-  using Cfg = DecCfg<T>;
   constexpr int W = Cfg::warps;
   extern __shared__ __align__(16) uint32_t dec_smem[];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   uint32_t *const sw = dec_smem + warp * Cfg::words;
   Control *ctl = a.ctl;
+  if (PASS == kPassGeneral && ld_volatile(&ctl->deferred) == 0u) return;
   // ---- header (:1801-1828) ----
   if (a.bytes < Tr::hdr) { if (threadIdx.x == 0) set_status(ctl, kESTREAM); return; }
   const uint32_t dim = *reinterpret_cast<const uint32_t *>(a.s);
@@ -624,7 +666,7 @@ __global__ void __launch_bounds__(32 * DecCfg<T>::warps, DecCfg<T>::min_ctas) de
   for (; c < G; c += nwarps) {
     const uint32_t mwc = mw;
     if (c + nwarps < G) mw = dec_meta_word<T>(a.s, G, c + nwarps, lane);  // next record, in flight meanwhile
-    decode_chunk<T, DIM>(a, c, n, G, pay_base, eb, seg, g, mwc, sw, lane);
+    decode_chunk<T, DIM, Cfg, PASS>(a, c, n, G, pay_base, eb, seg, g, mwc, sw, lane);
   }
 }
 

@@ -38,6 +38,7 @@ struct Control {
   double out_mm[6];                 // 96  rel->abs min/max
   uint64_t G;                       // 144 chunks (decompress: from the header)
   double strict_eb;                 // 152 bound actually encoded in strict-bound mode
+  uint32_t deferred;                // 160 decompress: chunks left to the general float64 pass
 };
 static_assert(sizeof(Control) <= kCtlBytes, "control block too large");
 

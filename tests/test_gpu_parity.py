@@ -230,6 +230,23 @@ def test_fallback_sort_sorted_input():
         assert s_g == s_o
 
 
+def test_float64_two_pass_decode_mixed_geometry():
+    """Float64 chunks of ordinary geometry are decoded in the compact layout;
+    chunks whose block-count product needs 64 bits are left to the general
+    pass.  A stream with both kinds, chunk-aligned halves."""
+    rng = np.random.default_rng(31)
+    n, half = 40 * 1024, 20 * 1024
+    axes = []
+    for _ in range(3):
+        a = np.empty(n, np.float64)
+        a[:half] = rng.uniform(500.0, 500.05, half)   # about 250 blocks per axis
+        a[half:] = rng.uniform(0.0, 1000.0, n - half)  # about 5e6 blocks per axis
+        axes.append(a)
+    run_arrays(axes[0], axes[1], axes[2], 3, 64, "abs", 1e-4, 1)
+    # and the general pass alone: every chunk wide
+    run_arrays(axes[0][half:].copy(), axes[1][half:].copy(), axes[2][half:].copy(), 3, 64, "abs", 1e-4, 1)
+
+
 def test_unaligned_soa_views():
     """x, y, z carved from one buffer with n % 4 != 0 (the plugin layout,
     src/main.cpp:283-334): 4-byte aligned only, scalar path."""
