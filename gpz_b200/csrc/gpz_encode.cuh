@@ -480,9 +480,8 @@ struct ChunkPoints {
 };
 
 // First phase of encoding chunk c: min/max, quantization, block ids (into q)
-// and relative positions (into the warp's third 4 KB, by rank r).  It touches
-// no other part of the warp's region, so it may run while the region's first
-// 8 KB still hold the previous chunk's staged payload.
+// and relative positions (into the warp's third 4 KB, by rank r); double
+// streams also stage each axis in the region's first 8 KB.
 template <typename T, int DIM>
 __device__ __forceinline__ void encode_quantize(const CArgs<T> &a, unsigned long long c, uint32_t *sw,
                                                 uint32_t seg, uint32_t sh, uint32_t msk, T eb, T inv,
@@ -503,20 +502,26 @@ __device__ __forceinline__ void encode_quantize(const CArgs<T> &a, unsigned long
   T mm[6];
   unsigned long long bnx = 0, bny = 0, bound = 0;
   uint32_t rmax = 0;
+  // Double streams stage each axis in the warp's first 8 KB (free while a
+  // chunk is quantized: the previous payload has been copied out), element j
+  // of lane l at word pair 32j + l, so the min/max and quantize passes read
+  // it back without holding 32 doubles in registers.
+  T *const stash = reinterpret_cast<T *>(sw);
 #pragma unroll
   for (int d = 0; d < DIM; ++d) {
-    T vl[ChunkPoints<T, DIM>::kAhead ? 1 : 32];
     if constexpr (!ChunkPoints<T, DIM>::kAhead) {
       const T *src = X[d] + base;
-#pragma unroll
+      if (d > 0) __syncwarp();  // the previous axis has been read
+#pragma unroll 8
       for (int j = 0; j < 32; ++j) {
         const uint32_t p = 32u * j + lane;
-        vl[j] = (full || p < nvalid) ? src[p] : src[0];  // past the end: the first point
+        stash[p] = (full || p < nvalid) ? src[p] : src[0];  // past the end: the first point
       }
+      __syncwarp();
     }
     auto vv_of = [&](int j) -> T {
       if constexpr (ChunkPoints<T, DIM>::kAhead) return pts.v[d][j];
-      else return vl[j];
+      else return stash[32u * j + lane];
     };
     // fmin / fmax ignore NaN and order -0.0 below +0.0, as the reference's
     // warp reductions do (:122-139); slots past the end repeat a point
