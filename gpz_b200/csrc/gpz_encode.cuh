@@ -22,11 +22,12 @@
 //   4. reports its payload size, then transposes deltas, counts and relative
 //      positions into bit planes in registers and assembles the payload in
 //      its shared region.
-// The 8 warps of a CTA take 8 consecutive chunks (a group) together, with no
-// CTA-wide barrier in the loop: the first warp to report a size claims the
-// next group, the first warp to finish its planes resolves the group's
-// stream offset (one decoupled look-back per group) while slower warps still
-// build theirs, and each warp copies its payload out once the offset is known.
+// The 8 warps of a CTA take 8 consecutive chunks (a group) together, with
+// three CTA barriers per group: B0 before the next group is claimed, B1 once
+// every payload size is known (warp 0 then publishes the group's aggregate),
+// B2 once warp 0, after building its own planes, has resolved the group's
+// stream offset (one decoupled look-back per group); each warp then copies
+// its payload out while the next chunk's loads are in flight.
 #pragma once
 
 #include <cfloat>
@@ -240,7 +241,8 @@ __device__ __forceinline__ void put_planes(uint32_t *stage, uint32_t pos0, uint3
 // Ranks a chunk whose composites (block id - kmin) << 10 | r need more than
 // 32 bits: 2048 buckets on the top bits (shared-atomic counts, placement by
 // bucket start + arrival slot), S keeping the bits below the bucket; buckets
-// of 2..15 points ordered by their owning lane, larger ones by the warp.  On
+// of 16 or more points are sorted by the warp, smaller ones by transposition
+// steps on the lanes' registers once the positions are loaded in order.  On
 // entry S's row l holds lane l's block ids; on exit S's row l holds the
 // sorted block ids of positions 32l..32l+31 and the first 16 words of hist's
 // row l the ranks r of positions j, j+16 as 16-bit pairs.
@@ -337,26 +339,6 @@ static __device__ __noinline__ void rank_wide(uint32_t *sw, uint32_t kmin, uint3
       if (en - st >= (uint32_t)kEncSmall) warp_bitonic_u32(S, st, en - st, lane);
     }
   }
-  {
-    // wide composites (S holds the bits below the bucket): each lane orders
-    // its own small buckets by insertion
-#pragma unroll 1
-    for (uint32_t b = 64u * lane; b < 64u * lane + 64u; ++b) {
-      const uint32_t st = bucket_start(hist, b, nvalid), en = bucket_start(hist, b + 1, nvalid);
-      if (en - st < 2u || en - st >= (uint32_t)kEncSmall) continue;
-      for (uint32_t i = st + 1; i < en; ++i) {
-        const uint32_t x = S[sx(i)];
-        uint32_t k2 = i;
-        while (k2 > st) {
-          const uint32_t y = S[sx(k2 - 1)];
-          if (y <= x) break;
-          S[sx(k2)] = y;
-          --k2;
-        }
-        S[sx(k2)] = x;
-      }
-    }
-  }
   __syncwarp();
 
   // sorted order: this lane's positions 32l..32l+31
@@ -366,8 +348,6 @@ static __device__ __noinline__ void rank_wide(uint32_t *sw, uint32_t kmin, uint3
       const uint4 t = *reinterpret_cast<const uint4 *>(S + qoff(lane, m));
       key[4 * m] = t.x; key[4 * m + 1] = t.y; key[4 * m + 2] = t.z; key[4 * m + 3] = t.w;
     }
-#pragma unroll
-    for (int k = 0; k < 16; ++k) rp[k] = (key[k] & 1023u) | ((key[k + 16] & 1023u) << 16);
     {
       // bucket of every position: max-scan of bucket indices written at the
       // bucket starts (the count words are done with)
@@ -407,8 +387,46 @@ static __device__ __noinline__ void rank_wide(uint32_t *sw, uint32_t kmin, uint3
       }
       uint32_t pre = __shfl_up_sync(FULL, inc, 1);
       if (lane == 0) pre = 0;
+      // positions past the chunk's end (stale words; the caller gives them
+      // the last id) take distinct out-of-range buckets, so no step moves them
 #pragma unroll
-      for (int j = 0; j < 32; ++j) key[j] = kmin + ((max(bpos[j], pre) << (shb - 10u)) | (key[j] >> 10));
+      for (int j = 0; j < 32; ++j)
+        bpos[j] = (full || 32u * lane + j < nvalid) ? max(bpos[j], pre) : (0x80000000u | (32u * lane + j));
+      // order inside the buckets of 2..15 points (they arrive in slot
+      // order; the big ones are sorted): odd-even transposition steps
+      // between neighbouring positions of one bucket, until a pair of steps
+      // swaps nothing; a bucket of n points is in order after n steps
+#pragma unroll 1
+      for (int it = 0; it < kEncSmall; ++it) {
+        bool swapped = false;
+#pragma unroll
+        for (int j = 0; j < 32; j += 2) {
+          const bool x = bpos[j] == bpos[j + 1] && key[j] > key[j + 1];
+          const uint32_t lo = x ? key[j + 1] : key[j], hi = x ? key[j] : key[j + 1];
+          key[j] = lo; key[j + 1] = hi;
+          swapped |= x;
+        }
+        const uint32_t nk = __shfl_down_sync(FULL, key[0], 1), nb = __shfl_down_sync(FULL, bpos[0], 1);
+        const uint32_t pk = __shfl_up_sync(FULL, key[31], 1), pb = __shfl_up_sync(FULL, bpos[31], 1);
+#pragma unroll
+        for (int j = 1; j < 31; j += 2) {
+          const bool x = bpos[j] == bpos[j + 1] && key[j] > key[j + 1];
+          const uint32_t lo = x ? key[j + 1] : key[j], hi = x ? key[j] : key[j + 1];
+          key[j] = lo; key[j + 1] = hi;
+          swapped |= x;
+        }
+        // the pair across lanes: position 32l+31 and 32(l+1); both lanes
+        // decide on the same two values
+        const bool xr = lane < 31 && nb == bpos[31] && key[31] > nk;
+        const bool xl = lane > 0 && pb == bpos[0] && pk > key[0];
+        if (xr) key[31] = nk;
+        if (xl) key[0] = pk;
+        if (!__any_sync(FULL, swapped || xr)) break;
+      }
+#pragma unroll
+      for (int k = 0; k < 16; ++k) rp[k] = (key[k] & 1023u) | ((key[k + 16] & 1023u) << 16);
+#pragma unroll
+      for (int j = 0; j < 32; ++j) key[j] = kmin + ((bpos[j] << (shb - 10u)) | (key[j] >> 10));
     }
   }
   __syncwarp();
