@@ -91,6 +91,7 @@ __global__ void __launch_bounds__(32 * kEncWarps, GPZ_ENC_MIN_CTAS)
   ChunkPoints<T, DIM> pts;
   pts.load(args[0], (eg.nmap & kLocal) * kEncWarps + warp, lane);
   int slot = 0;
+  uint32_t rank_skip = 0;
   for (;;) {
     const unsigned long long g = eg.next;
     if (g >= total) break;
@@ -119,7 +120,7 @@ __global__ void __launch_bounds__(32 * kEncWarps, GPZ_ENC_MIN_CTAS)
       }
     };
     uint32_t payload = 0, meta_word = 0;
-    if (live && c < G) payload = encode_chunk<T, DIM>(a, c, sw, seg, sh, msk, eb, inv, pts, meta_word, lane, on_size);
+    if (live && c < G) payload = encode_chunk<T, DIM>(a, c, sw, seg, sh, msk, eb, inv, pts, meta_word, lane, rank_skip, on_size);
     else on_size(0u);
     if (live && warp == 0) {
       unsigned long long excl = 0;

@@ -45,6 +45,7 @@ namespace gpzb {
 constexpr int kEncWarps = GPZ_ENC_WARPS;  // chunks (warps) per CTA
 constexpr int kEncBucketBits = 11;        // ranking buckets per chunk: 2048
 constexpr int kEncSmall = 16;             // buckets of this many points or more are sorted by the whole warp
+constexpr uint32_t kEncBucketBackoff = 8; // chunks ranked by the warp sort alone after a declined one
 constexpr int kEncWords = 3 * kChunk;     // per-warp shared words (12 KB)
 static_assert(kStageBytes <= kEncWords * 4, "payload staging must fit the warp region");
 
@@ -238,15 +239,22 @@ __device__ __forceinline__ void put_planes(uint32_t *stage, uint32_t pos0, uint3
   }
 }
 
-// Ranks a chunk whose composites (block id - kmin) << 10 | r need more than
-// 32 bits: 2048 buckets on the top bits (shared-atomic counts, placement by
-// bucket start + arrival slot), S keeping the bits below the bucket; buckets
-// of 16 or more points are sorted by the warp, smaller ones by transposition
-// steps on the lanes' registers once the positions are loaded in order.  On
-// entry S's row l holds lane l's block ids; on exit S's row l holds the
-// sorted block ids of positions 32l..32l+31 and the first 16 words of hist's
-// row l the ranks r of positions j, j+16 as 16-bit pairs.
-static __device__ __noinline__ void rank_wide(uint32_t *sw, uint32_t kmin, uint32_t cbits_all, uint32_t nvalid, int lane) {
+// Ranks the chunk's composites (block id - kmin) << 10 | r through 2048
+// buckets on their top bits: shared-atomic counts (the old count is the
+// point's arrival slot), an exclusive scan to bucket starts, placement at
+// bucket start + slot (S keeps the bits below the bucket), then the order
+// inside the buckets: buckets of 16 or more points by the warp's bitonic
+// sort in S, smaller ones by odd-even transposition steps on the lanes'
+// registers once the positions are loaded in order.  cbits is the
+// composites' width, at least 21.  With may_decline set (32-bit composites,
+// which the data-independent warp sort can rank instead) a chunk with a
+// bucket of 16 or more points is declined: false is returned before the
+// placement, with S unchanged.  On entry S's row l holds lane l's block ids;
+// after a true return S's row l holds the sorted block ids of positions
+// 32l..32l+31 and the first 16 words of hist's row l the ranks r of
+// positions j, j+16 as 16-bit pairs.
+static __device__ __noinline__ bool rank_buckets(uint32_t *sw, uint32_t kmin, uint32_t cbits, uint32_t nvalid,
+                                                 bool may_decline, int lane) {
   constexpr uint32_t FULL = 0xFFFFFFFFu;
   uint32_t *const S = sw, *const hist = sw + kChunk;
   const bool full = nvalid == (uint32_t)kChunk;
@@ -256,66 +264,61 @@ static __device__ __noinline__ void rank_wide(uint32_t *sw, uint32_t kmin, uint3
     const uint4 t = *reinterpret_cast<const uint4 *>(S + qoff(lane, m));
     key[4 * m] = t.x; key[4 * m + 1] = t.y; key[4 * m + 2] = t.z; key[4 * m + 3] = t.w;
   }
-  __syncwarp();
-  // wider composites: 2048 buckets on the top bits, S keeps the bits below
-  const uint32_t shb = cbits_all - kEncBucketBits;
 #pragma unroll
   for (int m = 0; m < 8; ++m) *reinterpret_cast<uint4 *>(hist + qoff(lane, m)) = make_uint4(0u, 0u, 0u, 0u);
   __syncwarp();
-  uint32_t bs[32];  // bucket << 10 | arrival slot
-  auto count_pass = [&](auto wide_c) {
-    constexpr bool WIDE = decltype(wide_c)::value;
+  // bucket = the top 11 of the cbits bits; vv = the bits below it
+  const uint32_t shb = cbits - kEncBucketBits, lowb = shb - 10u;
+  uint32_t bs[32];  // bucket << 10 | arrival slot, then position << 11 | bucket
 #pragma unroll
-    for (int j = 0; j < 32; ++j) {
-      const uint32_t koff = key[j] - kmin, r = 32u * lane + j;
-      uint32_t b, vv;
-      if constexpr (!WIDE) {
-        vv = (koff << 10) | r;
-        b = vv >> shb;
-      } else {
-        b = koff >> (shb - 10u);
-        vv = ((koff & ((1u << (shb - 10u)) - 1u)) << 10) | r;
-      }
-      key[j] = vv;
-      bs[j] = 0;
-      if (full || 32u * j + lane < nvalid) {
-        const uint32_t h = (b & 1u) << 4;
-        const uint32_t old = atomicAdd(&hist[sx(b >> 1)], 1u << h);
-        bs[j] = (b << 10) | ((old >> h) & 0x3FFu);
-      }
+  for (int j = 0; j < 32; ++j) {
+    const uint32_t koff = key[j] - kmin, b = koff >> lowb;
+    key[j] = ((koff & ((1u << lowb) - 1u)) << 10) | (32u * lane + j);
+    bs[j] = 0;
+    if (full || 32u * j + lane < nvalid) {
+      const uint32_t h = (b & 1u) << 4;
+      const uint32_t old = atomicAdd(&hist[sx(b >> 1)], 1u << h);
+      bs[j] = (b << 10) | ((old >> h) & 0x3FFu);
     }
-  };
-  count_pass(std::true_type{});
+  }
   __syncwarp();
   // exclusive scan of the bucket counts; lane l owns buckets 64l..64l+63
   uint32_t bigw = 0;  // bit k: a bucket of count word k holds 16 or more points
   {
-    uint32_t w[32];
+    // two passes over the lane's row (the counts, then the starts), so that
+    // only one quad of it is held beside key and bs
+    uint32_t tot = 0;
 #pragma unroll
     for (int m = 0; m < 8; ++m) {
       const uint4 t = *reinterpret_cast<const uint4 *>(hist + qoff(lane, m));
-      w[4 * m] = t.x; w[4 * m + 1] = t.y; w[4 * m + 2] = t.z; w[4 * m + 3] = t.w;
-    }
-    uint32_t tot = 0;
+      const uint32_t w4[4] = {t.x, t.y, t.z, t.w};
 #pragma unroll
-    for (int k = 0; k < 32; ++k) {
-      const uint32_t c0 = w[k] & 0xFFFFu;
-      if (w[k] & 0xFFF0FFF0u) bigw |= 1u << k;
-      const uint32_t st = tot | ((tot + c0) << 16);
-      tot += c0 + (w[k] >> 16);
-      w[k] = st;
+      for (int e = 0; e < 4; ++e) {
+        if (w4[e] & 0xFFF0FFF0u) bigw |= 1u << (4 * m + e);
+        tot += (w4[e] & 0xFFFFu) + (w4[e] >> 16);
+      }
     }
+    if (may_decline && __any_sync(FULL, bigw != 0u)) return false;
     uint32_t inc = tot;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
       const uint32_t t = __shfl_up_sync(FULL, inc, o);
       if (lane >= o) inc += t;
     }
-    const uint32_t b0 = inc - tot, b2 = b0 | (b0 << 16);
+    uint32_t run = inc - tot;
 #pragma unroll
-    for (int m = 0; m < 8; ++m)
-      *reinterpret_cast<uint4 *>(hist + qoff(lane, m)) =
-          make_uint4(w[4 * m] + b2, w[4 * m + 1] + b2, w[4 * m + 2] + b2, w[4 * m + 3] + b2);
+    for (int m = 0; m < 8; ++m) {
+      uint4 *const q4 = reinterpret_cast<uint4 *>(hist + qoff(lane, m));
+      const uint4 t = *q4;
+      uint32_t w4[4] = {t.x, t.y, t.z, t.w};
+#pragma unroll
+      for (int e = 0; e < 4; ++e) {
+        const uint32_t c0 = w4[e] & 0xFFFFu, c1 = w4[e] >> 16;
+        w4[e] = run | ((run + c0) << 16);
+        run += c0 + c1;
+      }
+      *q4 = make_uint4(w4[0], w4[1], w4[2], w4[3]);
+    }
   }
   __syncwarp();
   // place: bucket start + arrival slot; every point now lies inside its
@@ -324,7 +327,9 @@ static __device__ __noinline__ void rank_wide(uint32_t *sw, uint32_t kmin, uint3
   for (int j = 0; j < 32; ++j) {
     if (full || 32u * j + lane < nvalid) {
       const uint32_t b = bs[j] >> 10;
-      S[sx(bucket_start(hist, b, nvalid) + (bs[j] & 0x3FFu))] = key[j];
+      const uint32_t pos = ((hist[sx(b >> 1)] >> ((b & 1u) << 4)) & 0xFFFFu) + (bs[j] & 0x3FFu);
+      S[sx(pos)] = key[j];
+      bs[j] = (pos << 11) | b;
     }
   }
   __syncwarp();
@@ -340,94 +345,65 @@ static __device__ __noinline__ void rank_wide(uint32_t *sw, uint32_t kmin, uint3
     }
   }
   __syncwarp();
+  // the bucket of every position (the bucket starts are done with; a sort
+  // inside a big bucket keeps its positions' bucket)
+#pragma unroll
+  for (int j = 0; j < 32; ++j)
+    if (full || 32u * j + lane < nvalid) hist[sx(bs[j] >> 11)] = bs[j] & 0x7FFu;
+  __syncwarp();
 
   // sorted order: this lane's positions 32l..32l+31
   {
+    uint32_t bpos[32];
 #pragma unroll
     for (int m = 0; m < 8; ++m) {
       const uint4 t = *reinterpret_cast<const uint4 *>(S + qoff(lane, m));
       key[4 * m] = t.x; key[4 * m + 1] = t.y; key[4 * m + 2] = t.z; key[4 * m + 3] = t.w;
+      const uint4 u = *reinterpret_cast<const uint4 *>(hist + qoff(lane, m));
+      bpos[4 * m] = u.x; bpos[4 * m + 1] = u.y; bpos[4 * m + 2] = u.z; bpos[4 * m + 3] = u.w;
     }
-    {
-      // bucket of every position: max-scan of bucket indices written at the
-      // bucket starts (the count words are done with)
-      uint32_t st2[32];
-#pragma unroll
-      for (int m = 0; m < 8; ++m) {
-        const uint4 t = *reinterpret_cast<const uint4 *>(hist + qoff(lane, m));
-        st2[4 * m] = t.x; st2[4 * m + 1] = t.y; st2[4 * m + 2] = t.z; st2[4 * m + 3] = t.w;
-      }
-      const uint32_t next0 = __shfl_down_sync(FULL, st2[0] & 0xFFFFu, 1);
-      __syncwarp();
-#pragma unroll
-      for (int m = 0; m < 8; ++m) *reinterpret_cast<uint4 *>(hist + qoff(lane, m)) = make_uint4(0u, 0u, 0u, 0u);
-      __syncwarp();
-#pragma unroll
-      for (int k = 0; k < 32; ++k) {
-        const uint32_t s0 = st2[k] & 0xFFFFu, s1 = st2[k] >> 16;
-        const uint32_t e1 = k < 31 ? (st2[k + 1] & 0xFFFFu) : (lane < 31 ? next0 : nvalid);
-        if (s1 > s0) hist[sx(s0)] = 64u * lane + 2 * k;
-        if (e1 > s1) hist[sx(s1)] = 64u * lane + 2 * k + 1;
-      }
-      __syncwarp();
-      uint32_t mxb = 0, bpos[32];
-#pragma unroll
-      for (int m = 0; m < 8; ++m) {
-        const uint4 t = *reinterpret_cast<const uint4 *>(hist + qoff(lane, m));
-        mxb = max(mxb, t.x); bpos[4 * m] = mxb;
-        mxb = max(mxb, t.y); bpos[4 * m + 1] = mxb;
-        mxb = max(mxb, t.z); bpos[4 * m + 2] = mxb;
-        mxb = max(mxb, t.w); bpos[4 * m + 3] = mxb;
-      }
-      uint32_t inc = mxb;
-#pragma unroll
-      for (int o = 1; o < 32; o <<= 1) {
-        const uint32_t t = __shfl_up_sync(FULL, inc, o);
-        if (lane >= o) inc = max(inc, t);
-      }
-      uint32_t pre = __shfl_up_sync(FULL, inc, 1);
-      if (lane == 0) pre = 0;
-      // positions past the chunk's end (stale words; the caller gives them
-      // the last id) take distinct out-of-range buckets, so no step moves them
+    // positions past the chunk's end (stale words; the caller gives them the
+    // last id) take distinct out-of-range buckets, so no step moves them
+    if (!full) {
 #pragma unroll
       for (int j = 0; j < 32; ++j)
-        bpos[j] = (full || 32u * lane + j < nvalid) ? max(bpos[j], pre) : (0x80000000u | (32u * lane + j));
-      // order inside the buckets of 2..15 points (they arrive in slot
-      // order; the big ones are sorted): odd-even transposition steps
-      // between neighbouring positions of one bucket, until a pair of steps
-      // swaps nothing; a bucket of n points is in order after n steps
-#pragma unroll 1
-      for (int it = 0; it < kEncSmall; ++it) {
-        bool swapped = false;
-#pragma unroll
-        for (int j = 0; j < 32; j += 2) {
-          const bool x = bpos[j] == bpos[j + 1] && key[j] > key[j + 1];
-          const uint32_t lo = x ? key[j + 1] : key[j], hi = x ? key[j] : key[j + 1];
-          key[j] = lo; key[j + 1] = hi;
-          swapped |= x;
-        }
-        const uint32_t nk = __shfl_down_sync(FULL, key[0], 1), nb = __shfl_down_sync(FULL, bpos[0], 1);
-        const uint32_t pk = __shfl_up_sync(FULL, key[31], 1), pb = __shfl_up_sync(FULL, bpos[31], 1);
-#pragma unroll
-        for (int j = 1; j < 31; j += 2) {
-          const bool x = bpos[j] == bpos[j + 1] && key[j] > key[j + 1];
-          const uint32_t lo = x ? key[j + 1] : key[j], hi = x ? key[j] : key[j + 1];
-          key[j] = lo; key[j + 1] = hi;
-          swapped |= x;
-        }
-        // the pair across lanes: position 32l+31 and 32(l+1); both lanes
-        // decide on the same two values
-        const bool xr = lane < 31 && nb == bpos[31] && key[31] > nk;
-        const bool xl = lane > 0 && pb == bpos[0] && pk > key[0];
-        if (xr) key[31] = nk;
-        if (xl) key[0] = pk;
-        if (!__any_sync(FULL, swapped || xr)) break;
-      }
-#pragma unroll
-      for (int k = 0; k < 16; ++k) rp[k] = (key[k] & 1023u) | ((key[k + 16] & 1023u) << 16);
-#pragma unroll
-      for (int j = 0; j < 32; ++j) key[j] = kmin + ((bpos[j] << (shb - 10u)) | (key[j] >> 10));
+        if (32u * lane + j >= nvalid) bpos[j] = 0x80000000u | (32u * lane + j);
     }
+    // order inside the buckets of 2..15 points (they arrive in slot order;
+    // the big ones are sorted): odd-even transposition steps between
+    // neighbouring positions of one bucket, until a pair of steps swaps
+    // nothing; a bucket of n points is in order after n steps
+#pragma unroll 1
+    for (int it = 0; it < kEncSmall; ++it) {
+      bool swapped = false;
+#pragma unroll
+      for (int j = 0; j < 32; j += 2) {
+        const bool x = bpos[j] == bpos[j + 1] && key[j] > key[j + 1];
+        const uint32_t lo = x ? key[j + 1] : key[j], hi = x ? key[j] : key[j + 1];
+        key[j] = lo; key[j + 1] = hi;
+        swapped |= x;
+      }
+      const uint32_t nk = __shfl_down_sync(FULL, key[0], 1), nb = __shfl_down_sync(FULL, bpos[0], 1);
+      const uint32_t pk = __shfl_up_sync(FULL, key[31], 1), pb = __shfl_up_sync(FULL, bpos[31], 1);
+#pragma unroll
+      for (int j = 1; j < 31; j += 2) {
+        const bool x = bpos[j] == bpos[j + 1] && key[j] > key[j + 1];
+        const uint32_t lo = x ? key[j + 1] : key[j], hi = x ? key[j] : key[j + 1];
+        key[j] = lo; key[j + 1] = hi;
+        swapped |= x;
+      }
+      // the pair across lanes: positions 32l+31 and 32(l+1); both lanes
+      // decide on the same two values
+      const bool xr = lane < 31 && nb == bpos[31] && key[31] > nk;
+      const bool xl = lane > 0 && pb == bpos[0] && pk > key[0];
+      if (xr) key[31] = nk;
+      if (xl) key[0] = pk;
+      if (!__any_sync(FULL, swapped || xr)) break;
+    }
+#pragma unroll
+    for (int k = 0; k < 16; ++k) rp[k] = (key[k] & 1023u) | ((key[k + 16] & 1023u) << 16);
+#pragma unroll
+    for (int j = 0; j < 32; ++j) key[j] = kmin + ((bpos[j] << lowb) | (key[j] >> 10));
   }
   __syncwarp();
 #pragma unroll
@@ -437,6 +413,7 @@ static __device__ __noinline__ void rank_wide(uint32_t *sw, uint32_t kmin, uint3
   for (int m = 0; m < 4; ++m)
     *reinterpret_cast<uint4 *>(hist + qoff(lane, m)) = make_uint4(rp[4 * m], rp[4 * m + 1], rp[4 * m + 2], rp[4 * m + 3]);
   __syncwarp();
+  return true;
 }
 
 // A quantized chunk between the two encode phases: its 31-bit block ids
@@ -641,7 +618,8 @@ __device__ __forceinline__ void encode_quantize(const CArgs<T> &a, unsigned long
 // in meta_word (word k of the record in lane k).
 template <typename T, int DIM, class OnSize>
 __device__ __forceinline__ uint32_t encode_pack(const CArgs<T> &a, unsigned long long c, uint32_t *sw, ChunkQ &q,
-                                                uint32_t &meta_word, int lane, OnSize &&on_size) {
+                                                uint32_t &meta_word, int lane, uint32_t &rank_skip,
+                                                OnSize &&on_size) {
   using Tr = TT<T>;
   constexpr bool is64 = sizeof(T) == 8;
   constexpr uint32_t FULL = 0xFFFFFFFFu;
@@ -659,7 +637,41 @@ __device__ __forceinline__ uint32_t encode_pack(const CArgs<T> &a, unsigned long
   const unsigned long long cmax = ((unsigned long long)(kmax - kmin) << 10) | 1023ull;
   const uint32_t cbits_all = bitlen64(cmax);
   uint32_t rp[16];  // rank r of positions j and j+16 (16-bit pairs)
-  if (cbits_all <= 32u) {
+  // Buckets rank every chunk whose composites are wider than 32 bits, and
+  // the 32-bit ones of at least 21 bits unless they have a bucket of 16 or
+  // more points (then the chunk is declined and the warp sorts its next
+  // kEncBucketBackoff chunks directly); the data-independent warp sort ranks
+  // the rest.  Both give the same order.
+  bool ranked = false;
+  if (cbits_all > 32u || (cbits_all >= 21u && rank_skip == 0u)) {
+    // block ids in and results out through S and hist rows
+#pragma unroll
+    for (int m = 0; m < 8; ++m)
+      *reinterpret_cast<uint4 *>(S + qoff(lane, m)) = make_uint4(key[4 * m], key[4 * m + 1], key[4 * m + 2], key[4 * m + 3]);
+    ranked = rank_buckets(sw, kmin, max(cbits_all, 21u), nvalid, cbits_all <= 32u, lane);
+#pragma unroll
+    for (int m = 0; m < 8; ++m) {
+      const uint4 t = *reinterpret_cast<const uint4 *>(S + qoff(lane, m));
+      key[4 * m] = t.x; key[4 * m + 1] = t.y; key[4 * m + 2] = t.z; key[4 * m + 3] = t.w;
+    }
+    if (ranked) {
+      if (!full) {  // positions past the end carry the last id: they start no run
+#pragma unroll
+        for (int j = 0; j < 32; ++j) key[j] = 32u * lane + j < nvalid ? key[j] : kmax;
+      }
+#pragma unroll
+      for (int m = 0; m < 4; ++m) {
+        const uint4 t = *reinterpret_cast<const uint4 *>(hist + qoff(lane, m));
+        rp[4 * m] = t.x; rp[4 * m + 1] = t.y; rp[4 * m + 2] = t.z; rp[4 * m + 3] = t.w;
+      }
+    } else {
+      rank_skip = kEncBucketBackoff;
+      __syncwarp();  // S is read back before the warp sort writes it
+    }
+  } else if (rank_skip != 0u) {
+    --rank_skip;
+  }
+  if (!ranked) {
     // 32-bit composites: one data-independent warp sort.  Slots past the
     // chunk's end (point 32j + lane >= nvalid) take the largest
     // composite, (kmax - kmin) << 10 | 1023: no point of a short chunk has
@@ -681,30 +693,6 @@ __device__ __forceinline__ uint32_t encode_pack(const CArgs<T> &a, unsigned long
     for (int k = 0; k < 16; ++k) rp[k] = (key[k] & 1023u) | ((key[k + 16] & 1023u) << 16);
 #pragma unroll
     for (int j = 0; j < 32; ++j) key[j] = kmin + (key[j] >> 10);
-  } else {
-    // wider composites: the bucket path, outside the hot path's register
-    // budget; block ids in and results out through S and hist rows.  (A
-    // coarse 32-bit warp sort with the dropped id bits parked beside the
-    // relative positions, checked afterwards, measured slower on the wide
-    // lattices: 7.7 ms against 6.7 ms for 200M float64 FCC points.)
-#pragma unroll
-    for (int m = 0; m < 8; ++m)
-      *reinterpret_cast<uint4 *>(S + qoff(lane, m)) = make_uint4(key[4 * m], key[4 * m + 1], key[4 * m + 2], key[4 * m + 3]);
-    rank_wide(sw, kmin, cbits_all, nvalid, lane);
-#pragma unroll
-    for (int m = 0; m < 8; ++m) {
-      const uint4 t = *reinterpret_cast<const uint4 *>(S + qoff(lane, m));
-      key[4 * m] = t.x; key[4 * m + 1] = t.y; key[4 * m + 2] = t.z; key[4 * m + 3] = t.w;
-    }
-    if (!full) {  // positions past the end carry the last id: they start no run
-#pragma unroll
-      for (int j = 0; j < 32; ++j) key[j] = 32u * lane + j < nvalid ? key[j] : kmax;
-    }
-#pragma unroll
-    for (int m = 0; m < 4; ++m) {
-      const uint4 t = *reinterpret_cast<const uint4 *>(hist + qoff(lane, m));
-      rp[4 * m] = t.x; rp[4 * m + 1] = t.y; rp[4 * m + 2] = t.z; rp[4 * m + 3] = t.w;
-    }
   }
   __syncwarp();  // ranking scratch is done with
 
@@ -843,15 +831,16 @@ __device__ __forceinline__ uint32_t encode_pack(const CArgs<T> &a, unsigned long
 // Encodes chunk c into the warp's region `sw`; returns the payload bytes and
 // leaves the meta record in meta_word (word k of the record in lane k).
 // on_size(bytes) runs (warp-wide) as soon as the payload size is known, before
-// the bit planes are built.
+// the bit planes are built.  rank_skip is the warp's count of chunks still to
+// rank by the warp sort without trying the buckets first.
 template <typename T, int DIM, class OnSize>
 __device__ __forceinline__ uint32_t encode_chunk(const CArgs<T> &a, unsigned long long c, uint32_t *sw,
                                                  uint32_t seg, uint32_t sh, uint32_t msk, T eb, T inv,
                                                  ChunkPoints<T, DIM> &pts, uint32_t &meta_word, int lane,
-                                                 OnSize &&on_size) {
+                                                 uint32_t &rank_skip, OnSize &&on_size) {
   ChunkQ q;
   encode_quantize<T, DIM>(a, c, sw, seg, sh, msk, eb, inv, pts, q, lane);
-  return encode_pack<T, DIM>(a, c, sw, q, meta_word, lane, on_size);
+  return encode_pack<T, DIM>(a, c, sw, q, meta_word, lane, rank_skip, on_size);
 }
 
 // Copies a staged payload (whole words) to its place in the stream: four
@@ -936,6 +925,7 @@ __global__ void __launch_bounds__(32 * kEncWarps, GPZ_ENC_MIN_CTAS) compress_ker
   __syncthreads();
   ChunkPoints<T, DIM> pts;
   pts.load(a, eg.next + warp, lane);
+  uint32_t rank_skip = 0;
   for (;;) {
     const unsigned long long gbase = eg.next;
     if (gbase >= G) break;
@@ -954,7 +944,7 @@ __global__ void __launch_bounds__(32 * kEncWarps, GPZ_ENC_MIN_CTAS) compress_ker
       }
     };
     uint32_t payload = 0, meta_word = 0;
-    if (c < G) payload = encode_chunk<T, DIM>(a, c, sw, seg, sh, msk, eb, inv, pts, meta_word, lane, on_size);
+    if (c < G) payload = encode_chunk<T, DIM>(a, c, sw, seg, sh, msk, eb, inv, pts, meta_word, lane, rank_skip, on_size);
     else on_size(0u);
     if (warp == 0) {
       // resolved only now: the predecessors have had this group's plane
