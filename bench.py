@@ -566,11 +566,15 @@ def run_ours(args):
             "roofline": {"bound": "hbm", "kernel": f"compress_kernel<{tname},{dim}>", "achieved": round(achieved_c, 2),
                          "peak": peak, "peak_kind": peak_kind, "unit": "GB/s", "frac": round(achieved_c / peak, 4),
                          "traffic": traffic_c, "alg_bytes_per_launch": alg},
-            "roofline_decompress": {"bound": "hbm", "kernel": f"decompress_kernel<{tname},{dim}>",
+            "roofline_decompress": {"bound": "hbm",
+                                    "kernel": f"decompress_kernel<{tname},{dim}>" + ("" if bits == 32 else
+                                              " (fast pass + general pass)"),
                                     "achieved": round(achieved_d, 2), "peak": peak, "peak_kind": peak_kind,
                                     "unit": "GB/s", "frac": round(achieved_d / peak, 4), "traffic": traffic_d,
                                     "alg_bytes_per_launch": alg},
-            "gpu_launches": 3 * args.steps,
+            # seg_sample, compress and decompress per step (float64: the
+            # decompress fast pass and the general pass that follows it)
+            "gpu_launches": (3 if bits == 32 else 4) * args.steps,
             "clocks": clocks,
             "e2e": None if e2e_val is None else
                    {"value": round(e2e_val, 4), "unit": "GB/s", "h2d_bytes_per_step": inb + nb,

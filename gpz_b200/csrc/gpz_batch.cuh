@@ -188,12 +188,14 @@ __global__ void dbatch_header_kernel(DItem<T> *items, uint32_t K) {
 }
 
 // decompress_kernel over the chunks of many streams: warps stride over the
-// global chunk list, cmap[c] = stream << 40 | chunk within the stream.
-template <typename T, int DIM>
-__global__ void __launch_bounds__(32 * DecCfg<T>::warps, DecCfg<T>::min_ctas)
+// global chunk list, cmap[c] = stream << 40 | chunk within the stream.  The
+// passes are decompress_kernel's: float64 classes run the fast pass in the
+// 12 KB layout, then the general pass, which skips every stream whose fast
+// pass left no chunk.
+template <typename T, int DIM, class Cfg = DecCfg<T>, int PASS = kPassAll>
+__global__ void __launch_bounds__(32 * Cfg::warps, Cfg::min_ctas)
     decompress_batch_kernel(const DItem<T> *__restrict__ items, const unsigned long long *__restrict__ cmap,
                             unsigned long long total) {
-  using Cfg = DecCfg<T>;
   constexpr int W = Cfg::warps;
   constexpr unsigned long long kLocal = (1ull << kBatchLocalBits) - 1;
   extern __shared__ __align__(16) uint32_t dec_smem[];
@@ -204,6 +206,7 @@ __global__ void __launch_bounds__(32 * DecCfg<T>::warps, DecCfg<T>::min_ctas)
     const unsigned long long m = cmap[gc];
     const DItem<T> &it = items[m >> kBatchLocalBits];
     if (!it.ok) continue;
+    if (PASS == kPassGeneral && ld_volatile(&it.a.ctl->deferred) == 0u) continue;
     const DArgs<T> a = it.a;
     const unsigned long long c = m & kLocal, G = it.G;
     const uint32_t seg = it.seg;
@@ -212,7 +215,7 @@ __global__ void __launch_bounds__(32 * DecCfg<T>::warps, DecCfg<T>::min_ctas)
     g.sh = (uint32_t)__ffs((int)seg) - 1u;
     g.msk = seg - 1u;
     const uint32_t mwc = dec_meta_word<T>(a.s, G, c, lane);
-    decode_chunk<T, DIM>(a, c, it.n, G, it.pay_base, it.eb, seg, g, mwc, sw, lane);
+    decode_chunk<T, DIM, Cfg, PASS>(a, c, it.n, G, it.pay_base, it.eb, seg, g, mwc, sw, lane);
   }
 }
 

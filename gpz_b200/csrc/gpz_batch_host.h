@@ -25,7 +25,8 @@ struct ClassPlan {
   uint64_t work = 0;            // compress: 8-chunk groups; decompress: chunks
   uint64_t rel_blocks = 0;      // compress: rel->abs blocks of GPZ_FLAG_REL_ON_DEVICE items
   uint64_t table_off = 0, map_off = 0, rmap_off = 0;
-  int grid = 0;
+  int grid = 0;   // persistent grid (float64 decompress: of the fast pass)
+  int grid2 = 0;  // float64 decompress: grid of the general pass
 };
 
 struct Layout {

@@ -96,10 +96,10 @@ int compress_grid(uint64_t groups) {
   return o ? (int)std::min<uint64_t>(groups, (uint64_t)current_sms() * o) : -1;
 }
 
-template <typename T, int DIM>
+template <typename T, int DIM, class Cfg = DecCfg<T>, int PASS = kPassAll>
 int dec_grid(uint64_t chunks) {
-  constexpr int W = DecCfg<T>::warps;
-  const int o = resident_ctas(decompress_batch_kernel<T, DIM>, 32 * W, dec_smem_bytes<T>());
+  constexpr int W = Cfg::warps;
+  const int o = resident_ctas(decompress_batch_kernel<T, DIM, Cfg, PASS>, 32 * W, dec_smem_bytes_of<Cfg>());
   return o ? (int)std::min<uint64_t>((chunks + W - 1) / W, (uint64_t)current_sms() * o) : -1;
 }
 
@@ -120,8 +120,15 @@ void enqueue_dclass(const gpzb_host::ClassPlan &cp, uint8_t *dev, cudaStream_t s
   DItem<T> *tab = reinterpret_cast<DItem<T> *>(dev + cp.table_off);
   const uint32_t K = (uint32_t)cp.items.size();
   dbatch_header_kernel<T, DIM><<<(K + 127) / 128, 128, 0, st>>>(tab, K);
-  decompress_batch_kernel<T, DIM><<<cp.grid, 32 * DecCfg<T>::warps, dec_smem_bytes<T>(), st>>>(
-      tab, reinterpret_cast<const unsigned long long *>(dev + cp.map_off), cp.work);
+  const auto *map = reinterpret_cast<const unsigned long long *>(dev + cp.map_off);
+  if constexpr (sizeof(T) == 4) {
+    decompress_batch_kernel<T, DIM><<<cp.grid, 32 * DecCfg<T>::warps, dec_smem_bytes<T>(), st>>>(tab, map, cp.work);
+  } else {
+    decompress_batch_kernel<T, DIM, DecCfgF64Fast, kPassFast>
+        <<<cp.grid, 32 * DecCfgF64Fast::warps, dec_smem_bytes_of<DecCfgF64Fast>(), st>>>(tab, map, cp.work);
+    decompress_batch_kernel<T, DIM, DecCfg<T>, kPassGeneral>
+        <<<cp.grid2, 32 * DecCfg<T>::warps, dec_smem_bytes<T>(), st>>>(tab, map, cp.work);
+  }
 }
 
 }  // namespace
@@ -201,10 +208,16 @@ bool decompress_layout(const gpz_dbatch_item *items, uint32_t count, Layout &L) 
     switch (c) {
       case 0: cp.grid = dec_grid<float, 2>(cp.work); break;
       case 1: cp.grid = dec_grid<float, 3>(cp.work); break;
-      case 2: cp.grid = dec_grid<double, 2>(cp.work); break;
-      default: cp.grid = dec_grid<double, 3>(cp.work); break;
+      case 2:
+        cp.grid = dec_grid<double, 2, DecCfgF64Fast, kPassFast>(cp.work);
+        cp.grid2 = dec_grid<double, 2, DecCfg<double>, kPassGeneral>(cp.work);
+        break;
+      default:
+        cp.grid = dec_grid<double, 3, DecCfgF64Fast, kPassFast>(cp.work);
+        cp.grid2 = dec_grid<double, 3, DecCfg<double>, kPassGeneral>(cp.work);
+        break;
     }
-    if (cp.grid < 1) return false;
+    if (cp.grid < 1 || (c >= 2 && cp.grid2 < 1)) return false;
   }
   L.bytes = off;
   return true;

@@ -286,6 +286,8 @@ struct gpz_server {
           Lc.cls[c].grid = std::max(1, (int)((Lc.cls[c].grid + cfg.streams - 1) / cfg.streams));
         if (!di.empty() && Ld.cls[c].grid > 0)
           Ld.cls[c].grid = std::max(1, (int)((Ld.cls[c].grid + cfg.streams - 1) / cfg.streams));
+        if (!di.empty() && Ld.cls[c].grid2 > 0)
+          Ld.cls[c].grid2 = std::max(1, (int)((Ld.cls[c].grid2 + cfg.streams - 1) / cfg.streams));
       }
     }
     uint8_t *ws = arena.base + s.ws_off;
