@@ -230,6 +230,35 @@ def test_fallback_sort_sorted_input():
         assert s_g == s_o
 
 
+def test_ranking_paths_mixed_within_warps():
+    """Every warp encodes several chunks (5,860 chunks), and every third group of
+    8 chunks is heavy: 300 points of each chunk in one small cube, the rest
+    spread over the box.  The bucket ranking declines those chunks (a bucket
+    of 16 or more points with 32-bit composites) to the warp sort, and the
+    warp then ranks its next chunks by the warp sort directly before trying
+    buckets again; the stream must equal the oracle's byte for byte."""
+    n = 6_000_000
+    rng = np.random.default_rng(77)
+    x = (rng.random(n) * 1000.0).astype(np.float32)
+    y = (rng.random(n) * 1000.0).astype(np.float32)
+    z = (rng.random(n) * 1000.0).astype(np.float32)
+    for c in range(0, n, 1024):
+        if (c // 8192) % 3 != 0:
+            continue
+        m = min(300, n - c)
+        sel = c + rng.choice(min(1024, n - c), m, replace=False)
+        cx, cy, cz = rng.random(3) * 990.0
+        x[sel] = (cx + rng.random(m) * 0.3).astype(np.float32)
+        y[sel] = (cy + rng.random(m) * 0.3).astype(np.float32)
+        z[sel] = (cz + rng.random(m) * 0.3).astype(np.float32)
+    # segment 64: 157 blocks per axis, 32-bit composites of at least 21 bits
+    eb = float(np.float32(0.05))
+    s_o = po.compress(x, y, z, 3, eb, 64)
+    s_g, r = _gpu_compress(x, y, z, 3, eb, 64, "abs", 0.0)
+    assert r.status == 0 and s_g == s_o
+    _check_roundtrip(s_g, 3, 32)
+
+
 def test_float64_two_pass_decode_mixed_geometry():
     """Float64 chunks of ordinary geometry are decoded in the compact layout;
     chunks whose block-count product needs 64 bits are left to the general
