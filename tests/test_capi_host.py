@@ -65,10 +65,11 @@ def test_host_argument_errors_without_gpu():
     assert lib.gpz_result_post(16, None, None) == gz.GPZ_EINVAL  # no host result
 
 
-@pytest.mark.parametrize("check", ["fastdiv_check", "transpose_check", "network_check"])
+@pytest.mark.parametrize("check", ["fastdiv_check", "transpose_check", "network_check", "bucket_check"])
 def test_device_helpers_on_host(tmp_path, check):
-    """Exact dividers, bit-plane transposes and register sorting networks of the
-    kernels, compiled for the host and checked against plain arithmetic."""
+    """Exact dividers, bit-plane transposes, register sorting networks and the
+    bucket ranking's schedule of the kernels, compiled for the host and checked
+    against plain arithmetic."""
     exe = tmp_path / check
     subprocess.run(["nvcc", "-std=c++17", "-O2", "-gencode", "arch=compute_100a,code=sm_100a",
                     "-I", os.path.join(ROOT, "gpz_b200", "csrc"), "-I", os.path.join(ROOT, "include"),
