@@ -242,19 +242,24 @@ __device__ __forceinline__ void put_planes(uint32_t *stage, uint32_t pos0, uint3
 // Ranks the chunk's composites (block id - kmin) << 10 | r through 2048
 // buckets on their top bits: shared-atomic counts (the old count is the
 // point's arrival slot), an exclusive scan to bucket starts, placement at
-// bucket start + slot (S keeps the bits below the bucket), then the order
-// inside the buckets: buckets of 16 or more points by the warp's bitonic
-// sort in S, smaller ones by odd-even transposition steps on the lanes'
-// registers once the positions are loaded in order.  cbits is the
-// composites' width, at least 21.  With may_decline set (32-bit composites,
-// which the data-independent warp sort can rank instead) a chunk with a
-// bucket of 16 or more points is declined: false is returned before the
-// placement, with S unchanged.  On entry S's row l holds lane l's block ids;
-// after a true return S's row l holds the sorted block ids of positions
-// 32l..32l+31 and the first 16 words of hist's row l the ranks r of
-// positions j, j+16 as 16-bit pairs.
+// bucket start + slot, then the order inside the buckets by odd-even
+// transposition steps on the lanes' registers once the positions are loaded
+// in order.  cbits is the composites' width.
+//  * kNarrow (21 <= cbits <= 32): S holds whole composites, so neighbours of
+//    different buckets are already in order and the steps compare values
+//    alone.  A chunk with a bucket of 16 or more points is declined (the
+//    data-independent warp sort ranks it instead): false is returned before
+//    the placement, with S unchanged.
+//  * wide (cbits > 32): S keeps the bits below the bucket, the bucket of
+//    every position is scattered beside it, and the steps compare within a
+//    bucket only; buckets of 16 or more points are sorted by the warp's
+//    bitonic network in S first.
+// On entry S's row l holds lane l's block ids; after a true return S's row l
+// holds the sorted block ids of positions 32l..32l+31 and the first 16 words
+// of hist's row l the ranks r of positions j, j+16 as 16-bit pairs.
+template <bool kNarrow>
 static __device__ __noinline__ bool rank_buckets(uint32_t *sw, uint32_t kmin, uint32_t cbits, uint32_t nvalid,
-                                                 bool may_decline, int lane) {
+                                                 int lane) {
   constexpr uint32_t FULL = 0xFFFFFFFFu;
   uint32_t *const S = sw, *const hist = sw + kChunk;
   const bool full = nvalid == (uint32_t)kChunk;
@@ -267,13 +272,21 @@ static __device__ __noinline__ bool rank_buckets(uint32_t *sw, uint32_t kmin, ui
 #pragma unroll
   for (int m = 0; m < 8; ++m) *reinterpret_cast<uint4 *>(hist + qoff(lane, m)) = make_uint4(0u, 0u, 0u, 0u);
   __syncwarp();
-  // bucket = the top 11 of the cbits bits; vv = the bits below it
+  // bucket = the top 11 of the cbits bits; the value kept in S: the whole
+  // composite (narrow) or the bits below the bucket (wide)
   const uint32_t shb = cbits - kEncBucketBits, lowb = shb - 10u;
-  uint32_t bs[32];  // bucket << 10 | arrival slot, then position << 11 | bucket
+  uint32_t bs[32];  // bucket << 10 | arrival slot, then (wide) position << 11 | bucket
 #pragma unroll
   for (int j = 0; j < 32; ++j) {
-    const uint32_t koff = key[j] - kmin, b = koff >> lowb;
-    key[j] = ((koff & ((1u << lowb) - 1u)) << 10) | (32u * lane + j);
+    const uint32_t koff = key[j] - kmin;
+    uint32_t b;
+    if constexpr (kNarrow) {
+      key[j] = (koff << 10) | (32u * lane + j);
+      b = key[j] >> shb;
+    } else {
+      b = koff >> lowb;
+      key[j] = ((koff & ((1u << lowb) - 1u)) << 10) | (32u * lane + j);
+    }
     bs[j] = 0;
     if (full || 32u * j + lane < nvalid) {
       const uint32_t h = (b & 1u) << 4;
@@ -298,7 +311,7 @@ static __device__ __noinline__ bool rank_buckets(uint32_t *sw, uint32_t kmin, ui
         tot += (w4[e] & 0xFFFFu) + (w4[e] >> 16);
       }
     }
-    if (may_decline && __any_sync(FULL, bigw != 0u)) return false;
+    if (kNarrow && __any_sync(FULL, bigw != 0u)) return false;
     uint32_t inc = tot;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
@@ -333,8 +346,9 @@ static __device__ __noinline__ bool rank_buckets(uint32_t *sw, uint32_t kmin, ui
     }
   }
   __syncwarp();
-  // buckets of 16 or more points: the whole warp sorts each one
-  while (__any_sync(FULL, bigw != 0)) {
+  // buckets of 16 or more points (wide composites only; narrow chunks with
+  // one were declined): the whole warp sorts each one
+  while (!kNarrow && __any_sync(FULL, bigw != 0)) {
     const int src = __ffs((int)__ballot_sync(FULL, bigw != 0)) - 1;
     const int k = __ffs((int)__shfl_sync(FULL, bigw, src)) - 1;
     if (lane == src) bigw &= bigw - 1;
@@ -345,29 +359,37 @@ static __device__ __noinline__ bool rank_buckets(uint32_t *sw, uint32_t kmin, ui
     }
   }
   __syncwarp();
-  // the bucket of every position (the bucket starts are done with; a sort
-  // inside a big bucket keeps its positions' bucket)
+  if constexpr (!kNarrow) {
+    // the bucket of every position (the bucket starts are done with; a sort
+    // inside a big bucket keeps its positions' bucket)
 #pragma unroll
-  for (int j = 0; j < 32; ++j)
-    if (full || 32u * j + lane < nvalid) hist[sx(bs[j] >> 11)] = bs[j] & 0x7FFu;
-  __syncwarp();
+    for (int j = 0; j < 32; ++j)
+      if (full || 32u * j + lane < nvalid) hist[sx(bs[j] >> 11)] = bs[j] & 0x7FFu;
+    __syncwarp();
+  }
 
   // sorted order: this lane's positions 32l..32l+31
   {
-    uint32_t bpos[32];
+    uint32_t bpos[32];  // wide: the bucket of each position
 #pragma unroll
     for (int m = 0; m < 8; ++m) {
       const uint4 t = *reinterpret_cast<const uint4 *>(S + qoff(lane, m));
       key[4 * m] = t.x; key[4 * m + 1] = t.y; key[4 * m + 2] = t.z; key[4 * m + 3] = t.w;
-      const uint4 u = *reinterpret_cast<const uint4 *>(hist + qoff(lane, m));
-      bpos[4 * m] = u.x; bpos[4 * m + 1] = u.y; bpos[4 * m + 2] = u.z; bpos[4 * m + 3] = u.w;
+      if constexpr (!kNarrow) {
+        const uint4 u = *reinterpret_cast<const uint4 *>(hist + qoff(lane, m));
+        bpos[4 * m] = u.x; bpos[4 * m + 1] = u.y; bpos[4 * m + 2] = u.z; bpos[4 * m + 3] = u.w;
+      }
     }
     // positions past the chunk's end (stale words; the caller gives them the
-    // last id) take distinct out-of-range buckets, so no step moves them
+    // last id) take the largest value (narrow) or distinct out-of-range
+    // buckets (wide), so no step moves them
     if (!full) {
 #pragma unroll
       for (int j = 0; j < 32; ++j)
-        if (32u * lane + j >= nvalid) bpos[j] = 0x80000000u | (32u * lane + j);
+        if (32u * lane + j >= nvalid) {
+          if constexpr (kNarrow) key[j] = 0xFFFFFFFFu;
+          else bpos[j] = 0x80000000u | (32u * lane + j);
+        }
     }
     // order inside the buckets of 2..15 points (they arrive in slot order;
     // the big ones are sorted): odd-even transposition steps between
@@ -378,24 +400,25 @@ static __device__ __noinline__ bool rank_buckets(uint32_t *sw, uint32_t kmin, ui
       bool swapped = false;
 #pragma unroll
       for (int j = 0; j < 32; j += 2) {
-        const bool x = bpos[j] == bpos[j + 1] && key[j] > key[j + 1];
+        const bool x = (kNarrow || bpos[j] == bpos[j + 1]) && key[j] > key[j + 1];
         const uint32_t lo = x ? key[j + 1] : key[j], hi = x ? key[j] : key[j + 1];
         key[j] = lo; key[j + 1] = hi;
         swapped |= x;
       }
-      const uint32_t nk = __shfl_down_sync(FULL, key[0], 1), nb = __shfl_down_sync(FULL, bpos[0], 1);
-      const uint32_t pk = __shfl_up_sync(FULL, key[31], 1), pb = __shfl_up_sync(FULL, bpos[31], 1);
+      const uint32_t nk = __shfl_down_sync(FULL, key[0], 1), pk = __shfl_up_sync(FULL, key[31], 1);
+      const uint32_t nb = kNarrow ? 0u : __shfl_down_sync(FULL, bpos[0], 1);
+      const uint32_t pb = kNarrow ? 0u : __shfl_up_sync(FULL, bpos[31], 1);
 #pragma unroll
       for (int j = 1; j < 31; j += 2) {
-        const bool x = bpos[j] == bpos[j + 1] && key[j] > key[j + 1];
+        const bool x = (kNarrow || bpos[j] == bpos[j + 1]) && key[j] > key[j + 1];
         const uint32_t lo = x ? key[j + 1] : key[j], hi = x ? key[j] : key[j + 1];
         key[j] = lo; key[j + 1] = hi;
         swapped |= x;
       }
       // the pair across lanes: positions 32l+31 and 32(l+1); both lanes
       // decide on the same two values
-      const bool xr = lane < 31 && nb == bpos[31] && key[31] > nk;
-      const bool xl = lane > 0 && pb == bpos[0] && pk > key[0];
+      const bool xr = lane < 31 && (kNarrow || nb == bpos[31]) && key[31] > nk;
+      const bool xl = lane > 0 && (kNarrow || pb == bpos[0]) && pk > key[0];
       if (xr) key[31] = nk;
       if (xl) key[0] = pk;
       if (!__any_sync(FULL, swapped || xr)) break;
@@ -403,7 +426,10 @@ static __device__ __noinline__ bool rank_buckets(uint32_t *sw, uint32_t kmin, ui
 #pragma unroll
     for (int k = 0; k < 16; ++k) rp[k] = (key[k] & 1023u) | ((key[k + 16] & 1023u) << 16);
 #pragma unroll
-    for (int j = 0; j < 32; ++j) key[j] = kmin + ((bpos[j] << lowb) | (key[j] >> 10));
+    for (int j = 0; j < 32; ++j) {
+      if constexpr (kNarrow) key[j] = kmin + (key[j] >> 10);
+      else key[j] = kmin + ((bpos[j] << lowb) | (key[j] >> 10));
+    }
   }
   __syncwarp();
 #pragma unroll
@@ -648,7 +674,8 @@ __device__ __forceinline__ uint32_t encode_pack(const CArgs<T> &a, unsigned long
 #pragma unroll
     for (int m = 0; m < 8; ++m)
       *reinterpret_cast<uint4 *>(S + qoff(lane, m)) = make_uint4(key[4 * m], key[4 * m + 1], key[4 * m + 2], key[4 * m + 3]);
-    ranked = rank_buckets(sw, kmin, max(cbits_all, 21u), nvalid, cbits_all <= 32u, lane);
+    ranked = cbits_all > 32u ? rank_buckets<false>(sw, kmin, cbits_all, nvalid, lane)
+                             : rank_buckets<true>(sw, kmin, cbits_all, nvalid, lane);
 #pragma unroll
     for (int m = 0; m < 8; ++m) {
       const uint4 t = *reinterpret_cast<const uint4 *>(S + qoff(lane, m));

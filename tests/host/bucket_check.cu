@@ -25,7 +25,10 @@ struct Out {
 };
 
 // ids[l][j]: block id of lane l's register j (point 32j + l, rank r = 32l + j).
-static Out emulate(const uint32_t (&ids)[32][32], uint32_t nvalid, bool may_decline) {
+// narrow: composites of at most 32 bits (whole composites in S, steps compare
+// values alone, a chunk with a big bucket is declined); otherwise the wide
+// form (the bits below the bucket in S, the bucket of each position beside).
+static Out emulate(const uint32_t (&ids)[32][32], uint32_t nvalid, bool narrow) {
   Out o;
   const bool full = nvalid == 1024u;
   uint32_t kmin = 0xFFFFFFFFu, kmax = 0;
@@ -47,14 +50,19 @@ static Out emulate(const uint32_t (&ids)[32][32], uint32_t nvalid, bool may_decl
     for (int t = 0; t < 32; ++t) {
       const int l = perm[t];
       const uint32_t koff = ids[l][j] - kmin;
-      b[l][j] = koff >> lowb;
-      vv[l][j] = ((koff & ((1u << lowb) - 1u)) << 10) | (32u * l + j);
+      if (narrow) {
+        vv[l][j] = (koff << 10) | (32u * l + j);
+        b[l][j] = vv[l][j] >> shb;
+      } else {
+        b[l][j] = koff >> lowb;
+        vv[l][j] = ((koff & ((1u << lowb) - 1u)) << 10) | (32u * l + j);
+      }
       if (full || 32u * j + l < nvalid) slot[l][j] = cnt[b[l][j]]++;
     }
   }
   bool big = false;
   for (uint32_t k = 0; k < 2048; ++k) big |= cnt[k] >= (uint32_t)gpzb::kEncSmall;
-  if (may_decline && big) { o.declined = true; return o; }
+  if (narrow && big) { o.declined = true; return o; }
   std::vector<uint32_t> start(2049, 0);
   for (uint32_t k = 0; k < 2048; ++k) start[k + 1] = start[k] + cnt[k];
   uint32_t S[1024], B[1024];
@@ -71,8 +79,9 @@ static Out emulate(const uint32_t (&ids)[32][32], uint32_t nvalid, bool may_decl
   uint32_t key[32][32], bpos[32][32];
   for (int l = 0; l < 32; ++l)
     for (int j = 0; j < 32; ++j) {
-      key[l][j] = S[32 * l + j];
-      bpos[l][j] = (full || 32u * l + j < nvalid) ? B[32 * l + j] : (0x80000000u | (32u * l + j));
+      const bool valid = full || 32u * l + j < nvalid;
+      key[l][j] = narrow && !valid ? 0xFFFFFFFFu : S[32 * l + j];
+      bpos[l][j] = narrow ? 0u : valid ? B[32 * l + j] : (0x80000000u | (32u * l + j));
     }
   bool any = true;
   for (int it = 0; it < gpzb::kEncSmall && any; ++it) {
@@ -102,7 +111,7 @@ static Out emulate(const uint32_t (&ids)[32][32], uint32_t nvalid, bool may_decl
   o.converged = !any;
   for (int l = 0; l < 32; ++l)
     for (int j = 0; j < 32; ++j) {
-      o.id[32 * l + j] = kmin + ((bpos[l][j] << lowb) | (key[l][j] >> 10));
+      o.id[32 * l + j] = narrow ? kmin + (key[l][j] >> 10) : kmin + ((bpos[l][j] << lowb) | (key[l][j] >> 10));
       o.r[32 * l + j] = key[l][j] & 1023u;
     }
   return o;
