@@ -11,12 +11,13 @@
 // and a point's register index is its rank within the lane.  The warp:
 //   1. loads and quantizes one axis at a time (block id in registers, the
 //      relative position accumulated in a shared row per lane);
-//   2. ranks the composites (block id - kmin) << 10 | r: when they fit in 32
-//      bits (the common case) by one data-independent warp sort of the 1024
-//      values (odd-even merge sort of each lane's 32, then bitonic merges
-//      across lanes on the transposed matrix); wider ones by 2048 buckets on
-//      the top bits (shared-atomic counts, placement by bucket start +
-//      arrival slot, multi-point buckets put in order afterwards);
+//   2. ranks the composites (block id - kmin) << 10 | r through 2048 buckets
+//      on their top bits (shared-atomic counts, placement by bucket start +
+//      arrival slot, multi-point buckets put in order afterwards) when they
+//      span 21 bits or more; a data-independent warp sort of the 1024 values
+//      (odd-even merge sort of each lane's 32, then bitonic merges across
+//      lanes on the transposed matrix) ranks narrower ones and the 32-bit
+//      chunks the buckets decline;
 //   3. finds the runs of equal ids (unique ids, deltas, counts) and compacts
 //      them through shared memory so lane l holds runs 32l..32l+31;
 //   4. reports its payload size, then transposes deltas, counts and relative
