@@ -298,10 +298,11 @@ static __device__ __noinline__ bool rank_buckets(uint32_t *sw, uint32_t kmin, ui
   __syncwarp();
   // exclusive scan of the bucket counts; lane l owns buckets 64l..64l+63
   uint32_t bigw = 0;  // bit k: a bucket of count word k holds 16 or more points
+  uint32_t rounds;    // transposition rounds the small buckets need
   {
     // two passes over the lane's row (the counts, then the starts), so that
     // only one quad of it is held beside key and bs
-    uint32_t tot = 0;
+    uint32_t tot = 0, mx2 = 0;
 #pragma unroll
     for (int m = 0; m < 8; ++m) {
       const uint4 t = *reinterpret_cast<const uint4 *>(hist + qoff(lane, m));
@@ -310,9 +311,14 @@ static __device__ __noinline__ bool rank_buckets(uint32_t *sw, uint32_t kmin, ui
       for (int e = 0; e < 4; ++e) {
         if (w4[e] & 0xFFF0FFF0u) bigw |= 1u << (4 * m + e);
         tot += (w4[e] & 0xFFFFu) + (w4[e] >> 16);
+        mx2 = __vmaxu2(mx2, w4[e]);
       }
     }
     if (kNarrow && __any_sync(FULL, bigw != 0u)) return false;
+    // a bucket of n points is in order after n alternating odd / even steps
+    // (whichever comes first), ceil(n / 2) rounds of the pair; buckets of 16
+    // or more are sorted already, so 8 rounds cover the rest
+    rounds = min((warp_max(max(mx2 & 0xFFFFu, mx2 >> 16)) + 1u) >> 1, (uint32_t)kEncSmall / 2u);
     uint32_t inc = tot;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
@@ -394,17 +400,14 @@ static __device__ __noinline__ bool rank_buckets(uint32_t *sw, uint32_t kmin, ui
     }
     // order inside the buckets of 2..15 points (they arrive in slot order;
     // the big ones are sorted): odd-even transposition steps between
-    // neighbouring positions of one bucket, until a pair of steps swaps
-    // nothing; a bucket of n points is in order after n steps
+    // neighbouring positions of one bucket, `rounds` pairs of steps
 #pragma unroll 1
-    for (int it = 0; it < kEncSmall; ++it) {
-      bool swapped = false;
+    for (uint32_t it = 0; it < rounds; ++it) {
 #pragma unroll
       for (int j = 0; j < 32; j += 2) {
         const bool x = (kNarrow || bpos[j] == bpos[j + 1]) && key[j] > key[j + 1];
         const uint32_t lo = x ? key[j + 1] : key[j], hi = x ? key[j] : key[j + 1];
         key[j] = lo; key[j + 1] = hi;
-        swapped |= x;
       }
       const uint32_t nk = __shfl_down_sync(FULL, key[0], 1), pk = __shfl_up_sync(FULL, key[31], 1);
       const uint32_t nb = kNarrow ? 0u : __shfl_down_sync(FULL, bpos[0], 1);
@@ -414,7 +417,6 @@ static __device__ __noinline__ bool rank_buckets(uint32_t *sw, uint32_t kmin, ui
         const bool x = (kNarrow || bpos[j] == bpos[j + 1]) && key[j] > key[j + 1];
         const uint32_t lo = x ? key[j + 1] : key[j], hi = x ? key[j] : key[j + 1];
         key[j] = lo; key[j + 1] = hi;
-        swapped |= x;
       }
       // the pair across lanes: positions 32l+31 and 32(l+1); both lanes
       // decide on the same two values
@@ -422,7 +424,6 @@ static __device__ __noinline__ bool rank_buckets(uint32_t *sw, uint32_t kmin, ui
       const bool xl = lane > 0 && (kNarrow || pb == bpos[0]) && pk > key[0];
       if (xr) key[31] = nk;
       if (xl) key[0] = pk;
-      if (!__any_sync(FULL, swapped || xr)) break;
     }
 #pragma unroll
     for (int k = 0; k < 16; ++k) rp[k] = (key[k] & 1023u) | ((key[k + 16] & 1023u) << 16);

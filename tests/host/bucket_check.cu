@@ -5,9 +5,10 @@
 // warp's bitonic network), then the odd-even transposition steps between
 // neighbouring positions of one bucket, with the pair across lanes -- and
 // compared with a plain sort of the composites (block id - kmin) << 10 | r.
-// Also checks that a chunk is declined exactly when it has a big bucket and
-// that the steps stop (no swap) before their bound.  Compiled with nvcc, runs
-// on the CPU.
+// The transposition runs ceil(largest bucket / 2) rounds, at most 8; an
+// exhaustive check confirms that n alternating steps sort n values whichever
+// parity comes first.  Also checks that a chunk is declined exactly when it
+// has a big bucket.  Compiled with nvcc, runs on the CPU.
 #include <algorithm>
 #include <cstdio>
 #include <cstdint>
@@ -19,8 +20,7 @@ static uint32_t rnd() { s ^= s << 13; s ^= s >> 7; s ^= s << 17; return (uint32_
 
 struct Out {
   bool declined = false;
-  int steps = 0;          // transposition iterations that ran
-  bool converged = true;  // the last iteration swapped nothing
+  int steps = 0;  // transposition rounds that ran
   uint32_t id[1024], r[1024];
 };
 
@@ -83,13 +83,15 @@ static Out emulate(const uint32_t (&ids)[32][32], uint32_t nvalid, bool narrow) 
       key[l][j] = narrow && !valid ? 0xFFFFFFFFu : S[32 * l + j];
       bpos[l][j] = narrow ? 0u : valid ? B[32 * l + j] : (0x80000000u | (32u * l + j));
     }
-  bool any = true;
-  for (int it = 0; it < gpzb::kEncSmall && any; ++it) {
-    any = false;
+  // rounds: ceil(largest bucket / 2), at most 8 (bigger buckets are sorted)
+  uint32_t maxb = 0;
+  for (uint32_t k = 0; k < 2048; ++k) maxb = std::max(maxb, cnt[k]);
+  const uint32_t rounds = std::min((maxb + 1u) >> 1, (uint32_t)gpzb::kEncSmall / 2u);
+  for (uint32_t it = 0; it < rounds; ++it) {
     ++o.steps;
     for (int l = 0; l < 32; ++l)
       for (int j = 0; j < 32; j += 2)
-        if (bpos[l][j] == bpos[l][j + 1] && key[l][j] > key[l][j + 1]) { std::swap(key[l][j], key[l][j + 1]); any = true; }
+        if (bpos[l][j] == bpos[l][j + 1] && key[l][j] > key[l][j + 1]) std::swap(key[l][j], key[l][j + 1]);
     uint32_t nk[32], nb[32], pk[32], pb[32];
     for (int l = 0; l < 32; ++l) {  // the shuffles read before the odd step
       nk[l] = key[(l + 1) & 31][0]; nb[l] = bpos[(l + 1) & 31][0];
@@ -97,18 +99,17 @@ static Out emulate(const uint32_t (&ids)[32][32], uint32_t nvalid, bool narrow) 
     }
     for (int l = 0; l < 32; ++l)
       for (int j = 1; j < 31; j += 2)
-        if (bpos[l][j] == bpos[l][j + 1] && key[l][j] > key[l][j + 1]) { std::swap(key[l][j], key[l][j + 1]); any = true; }
+        if (bpos[l][j] == bpos[l][j + 1] && key[l][j] > key[l][j + 1]) std::swap(key[l][j], key[l][j + 1]);
     bool xr[32], xl[32];
     for (int l = 0; l < 32; ++l) {
       xr[l] = l < 31 && nb[l] == bpos[l][31] && key[l][31] > nk[l];
       xl[l] = l > 0 && pb[l] == bpos[l][0] && pk[l] > key[l][0];
     }
     for (int l = 0; l < 32; ++l) {
-      if (xr[l]) { key[l][31] = nk[l]; any = true; }
+      if (xr[l]) key[l][31] = nk[l];
       if (xl[l]) key[l][0] = pk[l];
     }
   }
-  o.converged = !any;
   for (int l = 0; l < 32; ++l)
     for (int j = 0; j < 32; ++j) {
       o.id[32 * l + j] = narrow ? kmin + (key[l][j] >> 10) : kmin + ((bpos[l][j] << lowb) | (key[l][j] >> 10));
@@ -129,7 +130,7 @@ static long check(const uint32_t (&ids)[32][32], uint32_t nvalid, long &declined
     ++declined;
     return 0;
   }
-  long bad = !o.converged;
+  long bad = 0;
   maxsteps = std::max<long>(maxsteps, o.steps);
   std::vector<unsigned long long> ref;
   for (int l = 0; l < 32; ++l)
@@ -141,8 +142,29 @@ static long check(const uint32_t (&ids)[32][32], uint32_t nvalid, long &declined
   return bad;
 }
 
+// n alternating odd / even transposition steps sort n values, whichever parity
+// comes first: every permutation of n <= 9 distinct values.
+static long exhaustive_steps() {
+  long bad = 0;
+  for (int n = 1; n <= 9; ++n) {
+    int p[9];
+    for (int i = 0; i < n; ++i) p[i] = i;
+    do {
+      for (int first = 0; first < 2; ++first) {
+        int a[9];
+        std::copy(p, p + n, a);
+        for (int step = 0; step < n; ++step)
+          for (int i = (first + step) & 1; i + 1 < n; i += 2)
+            if (a[i] > a[i + 1]) std::swap(a[i], a[i + 1]);
+        for (int i = 0; i < n; ++i) bad += a[i] != i;
+      }
+    } while (std::next_permutation(p, p + n));
+  }
+  return bad;
+}
+
 int main() {
-  long bad = 0, checks = 0, declined = 0, maxsteps = 0;
+  long bad = exhaustive_steps(), checks = 0, declined = 0, maxsteps = 0;
   for (int it = 0; it < 20000; ++it) {
     uint32_t ids[32][32];
     const int kind = it % 5;
@@ -175,5 +197,5 @@ int main() {
     ++checks;
   }
   printf("checks=%ld declined=%ld max_steps=%ld bad=%ld\n", checks, declined, maxsteps, bad);
-  return bad != 0 || declined == 0 || maxsteps >= gpzb::kEncSmall;
+  return bad != 0 || declined == 0 || maxsteps > gpzb::kEncSmall / 2;
 }
