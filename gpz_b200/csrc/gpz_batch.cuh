@@ -51,8 +51,9 @@ __global__ void __launch_bounds__(256) batch_sample_kernel(const BItem<T> *items
                       (it.flags & kBatchSafe31) ? 1 : 0, it.a.ctl, blockIdx.x, gridDim.x);
 }
 
+template <int W>
 struct BatchGroup {
-  uint32_t sz[kEncWarps];     // payload bytes of each warp's chunk
+  uint32_t sz[W];             // payload bytes of each warp's chunk
   unsigned long long goff;    // stream offset of the group (~0: look-back gave up)
   unsigned long long next;    // next global group
   unsigned long long nmap;    // its map entry
@@ -63,9 +64,10 @@ struct BatchGroup {
 // current and the next group's snapshot live in shared memory (double
 // buffered: the next group's points are loaded before the current group's
 // copy-out).  A snapshot whose segment size could not be chosen (sampling
-// error, status set) is skipped as a whole.
-template <typename T, int DIM>
-__global__ void __launch_bounds__(32 * kEncWarps, GPZ_ENC_MIN_CTAS)
+// error, status set) is skipped as a whole.  Groups of W chunks, as in
+// compress_kernel<T, DIM>.
+template <typename T, int DIM, int W = enc_warps<T, DIM>()>
+__global__ void __launch_bounds__(32 * W, GPZ_ENC_MIN_CTAS)
     compress_batch_kernel(const BItem<T> *__restrict__ items, const unsigned long long *__restrict__ map,
                           unsigned long long total, unsigned long long *claim) {
   using Tr = TT<T>;
@@ -73,7 +75,7 @@ __global__ void __launch_bounds__(32 * kEncWarps, GPZ_ENC_MIN_CTAS)
   constexpr uint32_t FULL = 0xFFFFFFFFu;
   constexpr unsigned long long kLocal = (1ull << kBatchLocalBits) - 1;
   extern __shared__ __align__(16) uint32_t enc_smem[];
-  __shared__ BatchGroup eg;
+  __shared__ BatchGroup<W> eg;
   __shared__ CArgs<T> args[2];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   uint32_t *const sw = enc_smem + warp * kEncWords;
@@ -89,7 +91,7 @@ __global__ void __launch_bounds__(32 * kEncWarps, GPZ_ENC_MIN_CTAS)
   if (threadIdx.x == 0) claim_next(0);
   __syncthreads();
   ChunkPoints<T, DIM> pts;
-  pts.load(args[0], (eg.nmap & kLocal) * kEncWarps + warp, lane);
+  pts.load(args[0], (eg.nmap & kLocal) * W + warp, lane);
   int slot = 0;
   uint32_t rank_skip = 0;
   for (;;) {
@@ -101,7 +103,7 @@ __global__ void __launch_bounds__(32 * kEncWarps, GPZ_ENC_MIN_CTAS)
     const CArgs<T> &a = args[slot];
     Control *ctl = a.ctl;
     const unsigned long long G = a.G;
-    const unsigned long long gid = m & kLocal, gbase = gid * kEncWarps;
+    const unsigned long long gid = m & kLocal, gbase = gid * W;
     const uint32_t seg = ctl->seg;  // 0: the snapshot's sampling failed
     const bool live = seg != 0;
     const uint32_t sh = live ? (uint32_t)__ffs((int)seg) - 1u : 0u, msk = seg - 1u;
@@ -114,7 +116,7 @@ __global__ void __launch_bounds__(32 * kEncWarps, GPZ_ENC_MIN_CTAS)
       if (lane == 0) eg.sz[warp] = bytes;
       __syncthreads();  // B1: the group's sizes are known (and the next group's snapshot)
       if (live && warp == 0) {
-        const uint32_t s = lane < kEncWarps ? eg.sz[lane] : 0u;
+        const uint32_t s = lane < W ? eg.sz[lane] : 0u;
         tot = __reduce_add_sync(FULL, s);
         if (lane == 0) publish_aggregate(a.look, gid, tot);
       }
@@ -127,7 +129,7 @@ __global__ void __launch_bounds__(32 * kEncWarps, GPZ_ENC_MIN_CTAS)
       const bool ok = resolve_prefix(a.look, gid, tot, ctl, excl);
       if (lane == 0) eg.goff = ok ? excl : ~0ull;
     }
-    pts.load(args[slot ^ 1], (eg.nmap & kLocal) * kEncWarps + warp, lane);  // in flight during the copy-out
+    pts.load(args[slot ^ 1], (eg.nmap & kLocal) * W + warp, lane);  // in flight during the copy-out
     __syncthreads();  // B2: the group's stream offset is known
     const unsigned long long goff = eg.goff;
     if (live && c < G && goff != ~0ull) {

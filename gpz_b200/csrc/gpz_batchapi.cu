@@ -30,9 +30,13 @@ constexpr uint64_t kRelMaxBlocks = 1024;
 
 inline uint64_t align256(uint64_t v) { return (v + 255u) & ~255ull; }
 inline uint64_t chunks_of(uint64_t n) { return (n + kChunk - 1) / kChunk; }
-inline uint64_t groups_of(uint64_t n) { return (chunks_of(n) + kEncWarps - 1) / kEncWarps; }
 inline uint64_t rel_blocks_of(uint64_t n) { return std::min(kRelMaxBlocks, std::max<uint64_t>(1, n / kRelPointsPerBlock)); }
 int class_of(uint32_t bits, uint32_t dim) { return (bits == 64 ? 2 : 0) + (dim == 3 ? 1 : 0); }
+// chunks per group of a class's compress kernel (enc_warps of its float type and dimension)
+constexpr int class_warps(int c) {
+  return c == 0 ? enc_warps<float, 2>() : c == 1 ? enc_warps<float, 3>() : c == 2 ? enc_warps<double, 2>() : enc_warps<double, 3>();
+}
+inline uint64_t groups_of(uint64_t n, int c) { return (chunks_of(n) + class_warps(c) - 1) / class_warps(c); }
 
 template <typename T>
 void fill_item(BItem<T> &bi, const gpz_batch_item &it, uint8_t *dev, uint64_t ctl_off, uint64_t rctl_off,
@@ -92,7 +96,8 @@ __global__ void __launch_bounds__(256) batch_rel_mapped_kernel(BItem<T> *items, 
 // kernel's shared-memory attribute cannot be raised there).
 template <typename T, int DIM>
 int compress_grid(uint64_t groups) {
-  const int o = resident_ctas(compress_batch_kernel<T, DIM>, 32 * kEncWarps, enc_smem_bytes());
+  constexpr int W = enc_warps<T, DIM>();
+  const int o = resident_ctas(compress_batch_kernel<T, DIM>, 32 * W, enc_smem_bytes<W>());
   return o ? (int)std::min<uint64_t>(groups, (uint64_t)current_sms() * o) : -1;
 }
 
@@ -110,7 +115,8 @@ void enqueue_class(const gpzb_host::ClassPlan &cp, uint8_t *dev, uint64_t claim_
     batch_rel_mapped_kernel<T><<<(unsigned)cp.rel_blocks, 256, 0, st>>>(
         tab, reinterpret_cast<const unsigned long long *>(dev + cp.rmap_off));
   batch_sample_kernel<T><<<dim3(128, (unsigned)cp.items.size()), 256, 0, st>>>(tab);
-  compress_batch_kernel<T, DIM><<<cp.grid, 32 * kEncWarps, enc_smem_bytes(), st>>>(
+  constexpr int W = enc_warps<T, DIM>();
+  compress_batch_kernel<T, DIM><<<cp.grid, 32 * W, enc_smem_bytes<W>(), st>>>(
       tab, reinterpret_cast<const unsigned long long *>(dev + cp.map_off), cp.work,
       reinterpret_cast<unsigned long long *>(dev + claim_off));
 }
@@ -158,10 +164,11 @@ bool compress_layout(const gpz_batch_item *items, uint32_t count, Layout &L) {
   uint64_t off = 2ull * count * kCtlBytes;
   for (uint32_t i = 0; i < count; ++i) {
     L.look_off[i] = off;
-    off += 8 * groups_of(items[i].n);
-    ClassPlan &cp = L.cls[class_of(items[i].float_bits, items[i].dim)];
+    const int c = class_of(items[i].float_bits, items[i].dim);
+    off += 8 * groups_of(items[i].n, c);
+    ClassPlan &cp = L.cls[c];
     cp.items.push_back(i);
-    cp.work += groups_of(items[i].n);
+    cp.work += groups_of(items[i].n, c);
     if (items[i].flags & GPZ_FLAG_REL_ON_DEVICE) cp.rel_blocks += rel_blocks_of(items[i].n);
   }
   L.claim_off = align256(off);
@@ -238,7 +245,7 @@ void compress_tables(const gpz_batch_item *items, const Layout &L, uint8_t *dev,
                                   ctl_off(L.count + i), L.look_off[i]);
       else fill_item<double>(reinterpret_cast<BItem<double> *>(H(cp.table_off))[k], it, dev, ctl_off(i),
                              ctl_off(L.count + i), L.look_off[i]);
-      const uint64_t groups = groups_of(it.n);
+      const uint64_t groups = groups_of(it.n, c);
       for (uint64_t q = 0; q < groups; ++q) map[g++] = ((unsigned long long)k << kBatchLocalBits) | q;
       if (it.flags & GPZ_FLAG_REL_ON_DEVICE) {
         const uint64_t nb = rel_blocks_of(it.n);

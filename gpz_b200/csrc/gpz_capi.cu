@@ -92,17 +92,20 @@ int compress_t(const gpz_params *p, const void *d_x, const void *d_y, const void
   a.eb_dev = eb_dev;
   a.dim = p->dim;
   a.vec_ok = aligned16(d_x) && aligned16(d_y) && (p->dim == 2 || aligned16(d_z));
-  // persistent grid: one CTA per kEncWarps chunks in flight
-  constexpr size_t smem = enc_smem_bytes();
+  // persistent grid: one CTA per W chunks in flight (W = enc_warps<T, DIM>)
   NvtxRange krange("run compress kernel");
-  auto launch = [&](auto kernel) -> bool {
-    const int occ = resident_ctas(kernel, 32 * kEncWarps, smem);
+  auto launch = [&](auto kernel, auto w) -> bool {
+    constexpr int W = decltype(w)::value;
+    constexpr size_t smem = enc_smem_bytes<W>();
+    const int occ = resident_ctas(kernel, 32 * W, smem);
     if (occ == 0) return false;
-    const uint64_t grid = std::min<uint64_t>((G + kEncWarps - 1) / kEncWarps, (uint64_t)num_sms() * occ);
-    kernel<<<(unsigned)grid, 32 * kEncWarps, smem, st>>>(a);
+    const uint64_t grid = std::min<uint64_t>((G + W - 1) / W, (uint64_t)num_sms() * occ);
+    kernel<<<(unsigned)grid, 32 * W, smem, st>>>(a);
     return true;
   };
-  if (!(p->dim == 3 ? launch(compress_kernel<T, 3>) : launch(compress_kernel<T, 2>))) return GPZ_ECUDA;
+  using W3 = std::integral_constant<int, enc_warps<T, 3>()>;
+  using W2 = std::integral_constant<int, enc_warps<T, 2>()>;
+  if (!(p->dim == 3 ? launch(compress_kernel<T, 3>, W3{}) : launch(compress_kernel<T, 2>, W2{}))) return GPZ_ECUDA;
   return cuda_status(cudaGetLastError());
 }
 

@@ -43,6 +43,9 @@ namespace gpzb {
 #ifndef GPZ_ENC_WARPS
 #define GPZ_ENC_WARPS 8
 #endif
+#ifndef GPZ_ENC_WARPS_F64_3D
+#define GPZ_ENC_WARPS_F64_3D 6
+#endif
 constexpr int kEncWarps = GPZ_ENC_WARPS;  // chunks (warps) per CTA
 constexpr int kEncBucketBits = 11;        // ranking buckets per chunk: 2048
 constexpr int kEncSmall = 16;             // buckets of this many points or more are sorted by the whole warp
@@ -50,14 +53,22 @@ constexpr uint32_t kEncBucketBackoff = 8; // chunks ranked by the warp sort alon
 constexpr int kEncWords = 3 * kChunk;     // per-warp shared words (12 KB)
 static_assert(kStageBytes <= kEncWords * 4, "payload staging must fit the warp region");
 
-// Per-CTA state of the group of kEncWarps consecutive chunks a CTA encodes.
-struct EncGroup {
-  uint32_t sz[kEncWarps];    // payload bytes of each warp's chunk
+// Chunks (warps) per CTA of compress_kernel<T, DIM>: float64 3D streams use
+// 6 (about 170 registers a thread, where 8 warps spill: FCC 200M 4.6 -> 4.1
+// ms), the others 8 (6 measured slower for float32 and float64 2D).
+template <typename T, int DIM>
+constexpr int enc_warps() { return (sizeof(T) == 8 && DIM == 3) ? GPZ_ENC_WARPS_F64_3D : kEncWarps; }
+
+// Per-CTA state of the group of W consecutive chunks a CTA encodes.
+template <int W>
+struct EncGroupT {
+  uint32_t sz[W];            // payload bytes of each warp's chunk
   unsigned long long goff;   // stream offset of the group (~0: look-back gave up)
   unsigned long long next;   // first chunk of the next group
 };
 
-constexpr size_t enc_smem_bytes() { return (size_t)kEncWarps * kEncWords * 4; }
+template <int W = kEncWarps>
+constexpr size_t enc_smem_bytes() { return (size_t)W * kEncWords * 4; }
 
 // Index of bucket-count word w, position / run u, ... in a swizzled 1024-word
 // array (rows of 32 words, 16-byte quads XORed by the row).
@@ -925,20 +936,20 @@ __device__ __forceinline__ void place_chunk(const CArgs<T> &a, unsigned long lon
   if (c == G - 1 && lane == 0) a.ctl->stream_bytes = pay_base + off + payload;
 }
 
-// Persistent compress kernel: every CTA encodes groups of kEncWarps
-// consecutive chunks, one chunk per warp.  Per group: the warps quantize,
+// Persistent compress kernel: every CTA encodes groups of W consecutive
+// chunks, one chunk per warp.  Per group: the warps quantize,
 // rank and find the runs of their chunks; their payload sizes are then known
 // (barrier B1) and warp 0 publishes the group's aggregate, so that later
 // groups' look-backs can pass it while the warps build their bit planes;
 // warp 0 then resolves the group's stream offset (decoupled look-back) and
 // after barrier B2 every warp copies its staged payload out.
-template <typename T, int DIM>
-__global__ void __launch_bounds__(32 * kEncWarps, GPZ_ENC_MIN_CTAS) compress_kernel(const CArgs<T> a) {
+template <typename T, int DIM, int W = enc_warps<T, DIM>()>
+__global__ void __launch_bounds__(32 * W, GPZ_ENC_MIN_CTAS) compress_kernel(const CArgs<T> a) {
   using Tr = TT<T>;
   constexpr bool is64 = sizeof(T) == 8;
   constexpr uint32_t FULL = 0xFFFFFFFFu;
   extern __shared__ __align__(16) uint32_t enc_smem[];
-  __shared__ EncGroup eg;
+  __shared__ EncGroupT<W> eg;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   uint32_t *const sw = enc_smem + warp * kEncWords;
   Control *ctl = a.ctl;
@@ -950,7 +961,7 @@ __global__ void __launch_bounds__(32 * kEncWarps, GPZ_ENC_MIN_CTAS) compress_ker
   const unsigned long long G = a.G;
   const unsigned long long pay_base = Tr::hdr + 8ull * G + (unsigned long long)Tr::meta * G;
 
-  if (threadIdx.x == 0) eg.next = atomicAdd(&ctl->chunk_ctr, (uint32_t)kEncWarps);
+  if (threadIdx.x == 0) eg.next = atomicAdd(&ctl->chunk_ctr, (uint32_t)W);
   __syncthreads();
   ChunkPoints<T, DIM> pts;
   pts.load(a, eg.next + warp, lane);
@@ -959,15 +970,15 @@ __global__ void __launch_bounds__(32 * kEncWarps, GPZ_ENC_MIN_CTAS) compress_ker
     const unsigned long long gbase = eg.next;
     if (gbase >= G) break;
     __syncthreads();  // B0: everyone has the group before it is replaced
-    if (threadIdx.x == 0) eg.next = ld_volatile(&ctl->abort) ? G : atomicAdd(&ctl->chunk_ctr, (uint32_t)kEncWarps);
+    if (threadIdx.x == 0) eg.next = ld_volatile(&ctl->abort) ? G : atomicAdd(&ctl->chunk_ctr, (uint32_t)W);
     const unsigned long long c = gbase + warp;
-    const unsigned long long gid = gbase / kEncWarps;
+    const unsigned long long gid = gbase / W;
     uint32_t total = 0;
     auto on_size = [&](uint32_t bytes) {
       if (lane == 0) eg.sz[warp] = bytes;
       __syncthreads();  // B1: the group's sizes are known
       if (warp == 0) {
-        const uint32_t s = lane < kEncWarps ? eg.sz[lane] : 0u;
+        const uint32_t s = lane < W ? eg.sz[lane] : 0u;
         total = __reduce_add_sync(FULL, s);
         if (lane == 0) publish_aggregate(a.look, gid, total);
       }
