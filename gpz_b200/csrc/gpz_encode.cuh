@@ -251,18 +251,20 @@ __device__ __forceinline__ void put_planes(uint32_t *stage, uint32_t pos0, uint3
   }
 }
 
-// Ranks the chunk's composites (block id - kmin) << 10 | r through 2048
-// buckets on their top bits: shared-atomic counts (the old count is the
-// point's arrival slot), an exclusive scan to bucket starts, placement at
-// bucket start + slot, then the order inside the buckets by odd-even
-// transposition steps on the lanes' registers once the positions are loaded
-// in order.  cbits is the composites' width.
-//  * kNarrow (21 <= cbits <= 32): S holds whole composites, so neighbours of
+// Ranks the chunk's composites (block id - kmin) << 10 | r through buckets
+// on their top bits: shared-atomic counts (the old count is the point's
+// arrival slot), an exclusive scan to bucket starts, placement at bucket
+// start + slot, then the order inside the buckets by odd-even transposition
+// steps on the lanes' registers once the positions are loaded in order.
+// cbits is the composites' width.
+//  * kNarrow (21 <= cbits <= 32): 1024 buckets with a 32-bit counter each
+//    (the fewest instructions per point); S holds whole composites, so neighbours of
 //    different buckets are already in order and the steps compare values
 //    alone.  A chunk with a bucket of 16 or more points is declined (the
 //    data-independent warp sort ranks it instead): false is returned before
 //    the placement, with S unchanged.
-//  * wide (cbits > 32): S keeps the bits below the bucket, the bucket of
+//  * wide (cbits > 32): 2048 buckets, two 16-bit counters a word (S keeps
+//    the bits below the bucket, and they must fit 32 bits); the bucket of
 //    every position is scattered beside it, and the steps compare within a
 //    bucket only; buckets of 16 or more points are sorted by the warp's
 //    bitonic network in S first.
@@ -284,30 +286,35 @@ static __device__ __noinline__ bool rank_buckets(uint32_t *sw, uint32_t kmin, ui
 #pragma unroll
   for (int m = 0; m < 8; ++m) *reinterpret_cast<uint4 *>(hist + qoff(lane, m)) = make_uint4(0u, 0u, 0u, 0u);
   __syncwarp();
-  // bucket = the top 11 of the cbits bits; the value kept in S: the whole
-  // composite (narrow) or the bits below the bucket (wide)
+  // narrow: 1024 buckets on the top 10 bits, one 32-bit counter each, S
+  // keeps the whole composite; wide: 2048 buckets on the top 11 bits, two
+  // 16-bit counters a word, S keeps the bits below the bucket
   const uint32_t shb = cbits - kEncBucketBits, lowb = shb - 10u;
-  uint32_t bs[32];  // bucket << 10 | arrival slot, then (wide) position << 11 | bucket
+  uint32_t bs[32];  // narrow: counter word << 10 | arrival slot; wide: bucket << 10 | arrival
+                    // slot, then position << 11 | bucket
 #pragma unroll
   for (int j = 0; j < 32; ++j) {
     const uint32_t koff = key[j] - kmin;
-    uint32_t b;
+    bs[j] = 0;
     if constexpr (kNarrow) {
       key[j] = (koff << 10) | (32u * lane + j);
-      b = key[j] >> shb;
+      if (full || 32u * j + lane < nvalid) {
+        const uint32_t w = sx(key[j] >> (shb + 1u));
+        bs[j] = (w << 10) | atomicAdd(&hist[w], 1u);
+      }
     } else {
-      b = koff >> lowb;
+      const uint32_t b = koff >> lowb;
       key[j] = ((koff & ((1u << lowb) - 1u)) << 10) | (32u * lane + j);
-    }
-    bs[j] = 0;
-    if (full || 32u * j + lane < nvalid) {
-      const uint32_t h = (b & 1u) << 4;
-      const uint32_t old = atomicAdd(&hist[sx(b >> 1)], 1u << h);
-      bs[j] = (b << 10) | ((old >> h) & 0x3FFu);
+      if (full || 32u * j + lane < nvalid) {
+        const uint32_t h = (b & 1u) << 4;
+        const uint32_t old = atomicAdd(&hist[sx(b >> 1)], 1u << h);
+        bs[j] = (b << 10) | ((old >> h) & 0x3FFu);
+      }
     }
   }
   __syncwarp();
-  // exclusive scan of the bucket counts; lane l owns buckets 64l..64l+63
+  // exclusive scan of the bucket counts; lane l owns counter words
+  // 32l..32l+31 (buckets 32l.. narrow, 64l.. wide)
   uint32_t bigw = 0;  // bit k: a bucket of count word k holds 16 or more points
   uint32_t rounds;    // transposition rounds the small buckets need
   {
@@ -320,9 +327,15 @@ static __device__ __noinline__ bool rank_buckets(uint32_t *sw, uint32_t kmin, ui
       const uint32_t w4[4] = {t.x, t.y, t.z, t.w};
 #pragma unroll
       for (int e = 0; e < 4; ++e) {
-        if (w4[e] & 0xFFF0FFF0u) bigw |= 1u << (4 * m + e);
-        tot += (w4[e] & 0xFFFFu) + (w4[e] >> 16);
-        mx2 = __vmaxu2(mx2, w4[e]);
+        if constexpr (kNarrow) {
+          if (w4[e] >= (uint32_t)kEncSmall) bigw |= 1u << (4 * m + e);
+          tot += w4[e];
+          mx2 = max(mx2, w4[e]);
+        } else {
+          if (w4[e] & 0xFFF0FFF0u) bigw |= 1u << (4 * m + e);
+          tot += (w4[e] & 0xFFFFu) + (w4[e] >> 16);
+          mx2 = __vmaxu2(mx2, w4[e]);
+        }
       }
     }
     if (kNarrow && __any_sync(FULL, bigw != 0u)) return false;
@@ -344,9 +357,15 @@ static __device__ __noinline__ bool rank_buckets(uint32_t *sw, uint32_t kmin, ui
       uint32_t w4[4] = {t.x, t.y, t.z, t.w};
 #pragma unroll
       for (int e = 0; e < 4; ++e) {
-        const uint32_t c0 = w4[e] & 0xFFFFu, c1 = w4[e] >> 16;
-        w4[e] = run | ((run + c0) << 16);
-        run += c0 + c1;
+        if constexpr (kNarrow) {
+          const uint32_t c0 = w4[e];
+          w4[e] = run;
+          run += c0;
+        } else {
+          const uint32_t c0 = w4[e] & 0xFFFFu, c1 = w4[e] >> 16;
+          w4[e] = run | ((run + c0) << 16);
+          run += c0 + c1;
+        }
       }
       *q4 = make_uint4(w4[0], w4[1], w4[2], w4[3]);
     }
@@ -357,10 +376,14 @@ static __device__ __noinline__ bool rank_buckets(uint32_t *sw, uint32_t kmin, ui
 #pragma unroll
   for (int j = 0; j < 32; ++j) {
     if (full || 32u * j + lane < nvalid) {
-      const uint32_t b = bs[j] >> 10;
-      const uint32_t pos = ((hist[sx(b >> 1)] >> ((b & 1u) << 4)) & 0xFFFFu) + (bs[j] & 0x3FFu);
-      S[sx(pos)] = key[j];
-      bs[j] = (pos << 11) | b;
+      if constexpr (kNarrow) {
+        S[sx(hist[bs[j] >> 10] + (bs[j] & 0x3FFu))] = key[j];
+      } else {
+        const uint32_t b = bs[j] >> 10;
+        const uint32_t pos = ((hist[sx(b >> 1)] >> ((b & 1u) << 4)) & 0xFFFFu) + (bs[j] & 0x3FFu);
+        S[sx(pos)] = key[j];
+        bs[j] = (pos << 11) | b;
+      }
     }
   }
   __syncwarp();

@@ -25,9 +25,10 @@ struct Out {
 };
 
 // ids[l][j]: block id of lane l's register j (point 32j + l, rank r = 32l + j).
-// narrow: composites of at most 32 bits (whole composites in S, steps compare
-// values alone, a chunk with a big bucket is declined); otherwise the wide
-// form (the bits below the bucket in S, the bucket of each position beside).
+// narrow: composites of at most 32 bits (1024 buckets, whole composites in S,
+// steps compare values alone, a chunk with a big bucket is declined);
+// otherwise the wide form (2048 buckets, the bits below the bucket in S, the
+// bucket of each position beside).
 static Out emulate(const uint32_t (&ids)[32][32], uint32_t nvalid, bool narrow) {
   Out o;
   const bool full = nvalid == 1024u;
@@ -50,9 +51,9 @@ static Out emulate(const uint32_t (&ids)[32][32], uint32_t nvalid, bool narrow) 
     for (int t = 0; t < 32; ++t) {
       const int l = perm[t];
       const uint32_t koff = ids[l][j] - kmin;
-      if (narrow) {
+      if (narrow) {  // 1024 buckets on the top 10 bits
         vv[l][j] = (koff << 10) | (32u * l + j);
-        b[l][j] = vv[l][j] >> shb;
+        b[l][j] = vv[l][j] >> (shb + 1u);
       } else {
         b[l][j] = koff >> lowb;
         vv[l][j] = ((koff & ((1u << lowb) - 1u)) << 10) | (32u * l + j);
