@@ -569,10 +569,21 @@ __device__ __forceinline__ void encode_quantize(const CArgs<T> &a, unsigned long
     if constexpr (!ChunkPoints<T, DIM>::kAhead) {
       const T *src = X[d] + base;
       if (d > 0) __syncwarp();  // the previous axis has been read
+      if (full && a.vec_ok) {
+        // a full chunk of 16-byte aligned axes: 16-byte asynchronous copies,
+        // 16 per lane, all in flight at once, no registers
+        const uint32_t s0 = (uint32_t)__cvta_generic_to_shared(stash) + 16u * lane;
+        const char *g0 = reinterpret_cast<const char *>(src) + 16u * lane;
+#pragma unroll
+        for (int i = 0; i < 16; ++i)
+          asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(s0 + 512u * i), "l"(g0 + 512u * i) : "memory");
+        asm volatile("cp.async.wait_all;" ::: "memory");
+      } else {
 #pragma unroll 8
-      for (int j = 0; j < 32; ++j) {
-        const uint32_t p = 32u * j + lane;
-        stash[p] = (full || p < nvalid) ? src[p] : src[0];  // past the end: the first point
+        for (int j = 0; j < 32; ++j) {
+          const uint32_t p = 32u * j + lane;
+          stash[p] = (full || p < nvalid) ? src[p] : src[0];  // past the end: the first point
+        }
       }
       __syncwarp();
     }
