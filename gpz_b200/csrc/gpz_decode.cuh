@@ -38,12 +38,18 @@ struct DArgs {
 //   P   per-position id (fast path: then running quotients) or run index
 //   R   per-position relative position word
 //   C   staged output rows
+// Float32 decoder CTAs: 8 warps x 2 per SM (16 warps, 128 registers, 192 KB
+// of shared memory); 4 x 4 measured 2.7 % slower on the 143.7M-point
+// snapshot, 6 x 3 (112 registers) and 2 x 8 slower still.
 #ifndef GPZ_DEC_MIN_CTAS_F32
-#define GPZ_DEC_MIN_CTAS_F32 4  // resident float32 decoder CTAs per SM the register budget is sized for
+#define GPZ_DEC_MIN_CTAS_F32 2  // resident float32 decoder CTAs per SM the register budget is sized for
+#endif
+#ifndef GPZ_DEC_WARPS_F32
+#define GPZ_DEC_WARPS_F32 8     // float32 decoder warps per CTA
 #endif
 template <typename T> struct DecCfg;
 template <> struct DecCfg<float> {
-  static constexpr int warps = 4, min_ctas = GPZ_DEC_MIN_CTAS_F32;
+  static constexpr int warps = GPZ_DEC_WARPS_F32, min_ctas = GPZ_DEC_MIN_CTAS_F32;
   static constexpr int A = 0, P = 0, TL = kChunk, TH = kChunk, R = kChunk, C = 2 * kChunk, words = 3 * kChunk;
 };
 template <> struct DecCfg<double> {
